@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the FibreNet step loop on B200: bead-steps/s.
+
+Default workload: the tensile test (1,000,000 beads = 20,000 fibres x 50,
+finite box 1000x1000x20 with x and z walls and periodic y, HR_FL springs with
+E = 1e3 and lognormal failure stress, HR angles, LJ contacts with cut-off
+2.5, clamps at x < 2 and x > 998, dt = 0.0005), generated from a fixed seed
+because the reference ships no models.  One bench step is one time step of
+RunSimulationLoop over all beads; the contact list is rebuilt every 8 steps
+as in the reference.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own kernels (FibreNet/kernel.cl compiled
+as C, oracle/_ref) on the host cores for the same workload and metric.
+With N > 1 (torchrun) every rank runs an independent replica: the path is one
+network and does not shard ("replicas only"); value = all ranks' bead-steps
+over the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bead-steps/s (tensile network, 1 B200 per replica)"
+UNIT = "bead-steps/s"
+WORKLOAD = "tensile_1M"
+OUTPUT_FREQ = 100  # the tensile test records reaction force / broken springs every 100 steps
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=40)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--fibres", type=int, default=20000)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=20.0)
+    return p.parse_args()
+
+
+def workload(fibres: int):
+    from fibrenet_b200 import generate as g
+    s = (fibres / 20000.0) ** 0.5
+    box = (1000.0 * s, 1000.0 * s, 20.0)
+    return g.tensile_network(seed=1, fibres=fibres, beads=50, box=box, clamp_lo=2.0,
+                             clamp_hi=box[0] - 2.0)
+
+
+def config_dict(m, args, extra=None):
+    d = {"workload": WORKLOAD if args.fibres == 20000 else f"tensile_{m.n_beads}",
+         "beads": m.n_beads, "springs": m.n_springs, "angles": m.n_angles,
+         "fibres": args.fibres, "beads_per_fibre": 50, "box": list(m.settings.box),
+         "bc": "finite x,z / periodic y", "contacts": "LJ eps 1 sigma 1 cut 2.5",
+         "dt": m.settings.dt, "grid_update_freq": m.settings.grid_update_freq,
+         "cell": m.settings.box_unit_cell, "seed": 1,
+         "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single",
+         "l2": "working set above 126 MB L2 (inputs larger than L2, no flush)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(m, half_pairs: float) -> float:
+    """Bytes one step must move (SURVEY 8(d) formula): per bead 4 state arrays
+    x 16 B read + written and 16 B of constants, per spring 16 B (+9 B HR_FL),
+    per angle 20 B, list offsets 4 B per bead, 4 B per half-list pair."""
+    import numpy as np
+    n_fl = int((np.asarray(m.s_type) == 1).sum())
+    return (m.n_beads * (4 * 16 * 2 + 16) + m.n_springs * 16 + n_fl * 9 + m.n_angles * 20
+            + (m.n_beads + 1) * 4 + half_pairs * 4)
+
+
+def layout_bytes(m, half_pairs: float) -> float:
+    """Bytes the step kernel's own layout moves at minimum (FP64 positions)."""
+    n, ns, na = m.n_beads, m.n_springs, m.n_angles
+    state = n * (2 * 32 + 2 * 32 + 2 * 16 + 2 * 16)  # pos, img double4 r/w; v_old, F float4 r/w
+    bonds = ns * (8 + 16 + 2) + na * (16 + 8 + 8 + 1)
+    incid = (n + 1) * 8 + 2 * ns * 4 + 3 * na * 4
+    lists = n * 4 + 2 * half_pairs * 4
+    return state + bonds + incid + lists
+
+
+def traffic_from_profiles():
+    path = os.path.join(ROOT, "profiles", "k_step_tensile_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_bead_step:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference_rate(model, seconds: float, threads: int | None = None, steps_cap: int = 10**9,
+                       warmup: int = 1):
+    """Reference kernels (oracle/_ref) on the host cores; a time-bounded
+    sample of whole steps.  Returns (bead-steps/s, steps, threads, kind)."""
+    threads = threads or os.cpu_count()
+    os.environ.setdefault("OMP_PROC_BIND", "true")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    m = model.fp32_representable()
+    # the reference has one global boundary type; walls on every axis is the
+    # closest it can express to the finite-x / periodic-y box
+    m.settings.periodic_mask = -1
+    m.settings.bc_type = 1
+    kind = "reference"
+    if po.ref_available():
+        sim = po.RefSim(m, threads=threads)
+    else:
+        kind = "port"
+        threads = 1
+        sim = po.OracleSim(m, po.MODE_REF)
+    for _ in range(warmup):
+        sim.run(1)
+    done = 0
+    t0 = time.perf_counter()
+    while done < steps_cap:
+        sim.run(8)  # one rebuild cycle (grid_update_freq 8)
+        done += 8
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return m.n_beads * done / dt, done, threads, kind
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    m = workload(args.fibres)
+    budget = max(30.0, min(150.0, 3.0 * (args.steps + args.warmup)))
+    rate, done, threads, kind = cpu_reference_rate(m, budget, steps_cap=args.steps,
+                                                   warmup=min(args.warmup, 2))
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
+            "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * m.n_beads / rate,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": config_dict(m, args, {"boundary_in_reference": "walls on all axes"}),
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{done} whole steps of the full {m.n_beads}-bead network "
+                                       f"(time-bounded, {budget:.0f} s)"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from fibrenet_b200.native import Simulation
+
+    m = workload(args.fibres)
+    sim = Simulation(m, device=local, list_capacity=64, cell_capacity=64, reorder=True)
+    nb = m.n_beads
+
+    sim.step(max(args.warmup, 3))
+    sim.sync()
+    sim.rebuild()
+    cnt, _ = sim.lists()
+    half_pairs = float(cnt.sum()) / 2.0
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: device-resident state, K steps in one RunSimulationLoop call
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    sim.enable_timing(True)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record()
+    sim.step(args.steps)
+    sim.sync()
+    t1.record()
+    torch.cuda.synchronize()
+    elapsed_ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    kt = sim.kernel_time()
+    sim.enable_timing(False)
+    barrier()
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = world * nb * args.steps / (elapsed_ms / 1e3)
+    stats = sim.stats()
+    launches = 1 + args.steps + kt["rebuilds"] * 7
+
+    # ---- end to end through the public API: model upload from pinned host
+    # buffers, RunSimulationLoop in output_freq chunks with the recorded
+    # observables read back after each chunk, final state download
+    e2e_steps = args.steps
+    pinned = {}
+    mm = m.normalised()
+    for name in ["pos", "img", "vel", "vel_old", "force"]:
+        t = torch.from_numpy(getattr(mm, name)).pin_memory()
+        pinned[name] = t
+        setattr(mm, name, t.numpy())
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    w0 = time.perf_counter()
+    sim2 = Simulation(mm, device=local, list_capacity=64, cell_capacity=64, reorder=True)
+    done = 0
+    obs_bytes = 0
+    while done < e2e_steps:
+        k = min(OUTPUT_FREQ, e2e_steps - done)
+        sim2.step(k)
+        o = sim2.observe(0, reaction_type=2)
+        obs_bytes += 5 * 8
+        done += k
+    final = sim2.get("pos")
+    sim2.sync()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - w0
+    e2e_ms = max(e0.elapsed_time(e1), 1e3 * e2e_wall)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = sum(getattr(mm, k).nbytes for k in ["pos", "img", "vel", "vel_old", "force", "radius", "mass",
+                                            "type", "tag", "loc_id", "s_type", "s_p1", "s_p2",
+                                            "s_rest", "s_k", "s_c1", "s_c2", "a_type", "a_b1",
+                                            "a_b2", "a_b3", "a_s1", "a_s2", "a_theta0", "a_k"])
+    d2h = obs_bytes + final.nbytes
+    e2e_value = world * nb * e2e_steps / (e2e_ms / 1e3)
+    sim2.close()
+
+    peak, peak_kind = peaks()
+    alg = algorithmic_bytes(m, half_pairs)
+    step_ms = kt["step_ms"]
+    achieved = alg / (step_ms / 1e3) / 1e9 if step_ms > 0 else None
+    traffic_per_bead = traffic_from_profiles()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, done_cpu, threads, kind = cpu_reference_rate(m, args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{done_cpu} whole steps of the same {nb}-bead network on the host "
+                         f"(reference kernels as C, OpenMP, walls on all axes)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator; reference ships no models)",
+            "config": config_dict(m, args, {"half_list_pairs": half_pairs,
+                                            "storage": "positions f64, velocities/forces f32"}),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "peak_kind": peak_kind,
+                         "kernel": "k_step (force + kick + drift, one launch per step)",
+                         "algorithmic_bytes_per_launch": alg,
+                         "layout_bytes_per_launch": layout_bytes(m, half_pairs),
+                         "step_kernel_ms": step_ms, "rebuild_ms": kt["rebuild_ms"],
+                         "traffic": (traffic_per_bead * nb) if traffic_per_bead else None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+                    "d2h_bytes_per_step": d2h / e2e_steps,
+                    "what": "Simulation(model from pinned host arrays) + step() in chunks of "
+                            f"{OUTPUT_FREQ} with observe() after each + final get('pos')"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "overflow": {"cell": stats["cell_overflow"], "list": stats["list_overflow"]},
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

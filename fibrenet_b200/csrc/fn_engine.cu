@@ -1,0 +1,1149 @@
+/*
+ * fn_engine.cu -- host side of the C ABI (include/fibrenet.h).
+ *
+ * One fn_ctx replaces the reference's OpenclManager + BufferIndex pair
+ * (OpenclManager.h:20-174, BufferIndex.h:7-22): it owns the device buffers,
+ * derives the kernel constants from the input-file settings the way
+ * SimulationManager does, renumbers beads for locality, and sequences the
+ * step kernels on one stream (RunSimulationLoop, SimulationManager.cpp:151-181).
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/fibrenet.h"
+#include "fn_kernels.h"
+#include "fn_types.h"
+
+namespace {
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+};
+
+/* Per-network host bookkeeping. */
+struct NetHost {
+    int bead_begin, bead_end;
+    int spring_begin, spring_end;
+    int angle_begin, angle_end;
+    long long cell_begin, cell_end;
+    int grid_update_freq;
+    double damping;
+};
+
+int getadress_h(int t1, int t2, int size) {
+    return (t1 < t2) ? ((size * t1) + t2 - ((t1 * (t1 + 1)) / 2))
+                     : ((size * t2) + t1 - ((t2 * (t2 + 1)) / 2));
+}
+
+uint32_t spread10(uint32_t v) {
+    v &= 0x3ff;
+    v = (v | (v << 16)) & 0x030000FF;
+    v = (v | (v << 8)) & 0x0300F00F;
+    v = (v | (v << 4)) & 0x030C30C3;
+    v = (v | (v << 2)) & 0x09249249;
+    return v;
+}
+
+}  // namespace
+
+struct fn_ctx {
+    fn_config cfg{};
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool uploaded = false;
+
+    int n_nets = 0;
+    std::vector<FnNet> nets_h;
+    std::vector<NetHost> info;
+    std::vector<FnPair> pairs_h;
+    long long nb = 0, ns = 0, na = 0, ncells = 0;
+    std::vector<int> perm;  // internal -> upload
+    std::vector<int> inv;   // upload -> internal
+    std::vector<double> mass_h, radius_h;
+    std::vector<float4> sp_par_h;  // upload order (springs are not renumbered)
+    std::vector<float2> an_par_h;
+    bool damp = false;
+    int grid_update_freq = 8;
+
+    DevBuf<double4> pos[2], img[2];
+    DevBuf<float4> vold, force, vel;
+    DevBuf<int4> binfo;
+    DevBuf<int2> sp_ends;
+    DevBuf<float4> sp_par;
+    DevBuf<signed char> sp_type, sp_status;
+    DevBuf<int4> an_b;
+    DevBuf<int2> an_s;
+    DevBuf<float2> an_par;
+    DevBuf<signed char> an_status;
+    DevBuf<int> sp_off, sp_ent, an_off, an_ent;
+    DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
+    DevBuf<int> scan_sums;
+    DevBuf<FnTile> tiles;
+    DevBuf<FnNet> nets;
+    DevBuf<FnPair> pairs;
+    DevBuf<unsigned long long> counters;
+    DevBuf<double> obs_partial, obs_out;
+    int list_stride = 0;
+    int cur = 0;
+    int block = 128;
+    int ntiles = 0;
+    long long device_bytes = 0;
+    long long steps_done = 0, rebuilds_done = 0;
+
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_step, ev_rebuild;
+    size_t ev_next = 0;
+};
+
+namespace {
+
+int fail(fn_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(c, e_ == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA,    \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(fn_ctx* c, DevBuf<T>& b, size_t n) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->device_bytes -= (long long)(b.n * sizeof(T));
+        b.p = nullptr;
+        b.n = 0;
+    }
+    size_t bytes = sizeof(T) * (n ? n : 1);
+    cudaError_t e = cudaMalloc((void**)&b.p, bytes);
+    if (e == cudaSuccess) {
+        b.n = n ? n : 1;
+        c->device_bytes += (long long)bytes;
+    }
+    return e;
+}
+
+template <class T>
+void dfree(fn_ctx* c, DevBuf<T>& b) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->device_bytes -= (long long)(b.n * sizeof(T));
+    }
+    b.p = nullptr;
+    b.n = 0;
+}
+
+template <class T>
+cudaError_t h2d(fn_ctx* c, DevBuf<T>& b, const std::vector<T>& v) {
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c->stream);
+}
+
+void free_all(fn_ctx* c) {
+    for (int k = 0; k < 2; ++k) {
+        dfree(c, c->pos[k]);
+        dfree(c, c->img[k]);
+    }
+    dfree(c, c->vold);
+    dfree(c, c->force);
+    dfree(c, c->vel);
+    dfree(c, c->binfo);
+    dfree(c, c->sp_ends);
+    dfree(c, c->sp_par);
+    dfree(c, c->sp_type);
+    dfree(c, c->sp_status);
+    dfree(c, c->an_b);
+    dfree(c, c->an_s);
+    dfree(c, c->an_par);
+    dfree(c, c->an_status);
+    dfree(c, c->sp_off);
+    dfree(c, c->sp_ent);
+    dfree(c, c->an_off);
+    dfree(c, c->an_ent);
+    dfree(c, c->cell_of);
+    dfree(c, c->cell_count);
+    dfree(c, c->cell_fill);
+    dfree(c, c->cell_start);
+    dfree(c, c->cell_beads);
+    dfree(c, c->list_count);
+    dfree(c, c->list);
+    dfree(c, c->scan_sums);
+    dfree(c, c->tiles);
+    dfree(c, c->nets);
+    dfree(c, c->pairs);
+    dfree(c, c->counters);
+    dfree(c, c->obs_partial);
+    dfree(c, c->obs_out);
+}
+
+/* Kernel constants of one network (SimulationManager.cpp:647-671, 684-720,
+   802-817, 2076-2190, 891-932). */
+int derive_net(fn_ctx* c, const fn_settings& s, FnNet& N, int net_index) {
+    char buf[256];
+    if (!(s.dt > 0.0)) {
+        snprintf(buf, sizeof buf, "network %d: 'step' must be positive", net_index);
+        return fail(c, FN_ERR_ARG, buf);
+    }
+    if (!(s.box_unit_cell > 0.0) || !(s.box[0] > 0.0) || !(s.box[1] > 0.0) || !(s.box[2] > 0.0)) {
+        snprintf(buf, sizeof buf, "network %d: box and unit cell must be positive", net_index);
+        return fail(c, FN_ERR_ARG, buf);
+    }
+    for (int a = 0; a < 3; ++a)
+        if (s.box[a] / s.box_unit_cell < 3.0) {
+            snprintf(buf, sizeof buf,
+                     "network %d: box must be at least three unit cells per axis "
+                     "(SimulationManager.cpp:2104-2109)",
+                     net_index);
+            return fail(c, FN_ERR_ARG, buf);
+        }
+    if (s.n_types <= 0) return fail(c, FN_ERR_ARG, "n_types must be positive");
+    std::memset(&N, 0, sizeof N);
+    N.dt = s.dt;
+    N.half_dt = s.dt * 0.5;
+    N.half_dt2 = s.dt * s.dt * 0.5;
+    N.lambda_dt = s.lambda;
+    N.lambda_dt *= s.dt;
+    N.damping = s.damping * -1.0;
+    for (int a = 0; a < 3; ++a) {
+        N.g[a] = s.gravity[a];
+        N.box[a] = s.box[a];
+    }
+    N.cutoff_sq = s.cutoff * s.cutoff;
+    N.wall_k = s.wall_k;
+    N.nx = (int)std::floor(s.box[0] / s.box_unit_cell);
+    N.ny = (int)std::floor(s.box[1] / s.box_unit_cell);
+    N.nz = (int)std::floor(s.box[2] / s.box_unit_cell);
+    N.nxy = N.nx * N.ny;
+    N.step[0] = s.box[0] / (double)(float)N.nx;
+    N.step[1] = s.box[1] / (double)(float)N.ny;
+    N.step[2] = s.box[2] / (double)(float)N.nz;
+    double mn = std::fmin(std::fmin(s.box[0], s.box[1]), s.box[2]) * 0.5;
+    N.half_box_sq = mn * mn;
+    if (s.periodic_mask < 0) {
+        N.periodic = s.bc_type == 0 ? 7 : 0;
+        N.list_mi = N.periodic;
+        N.force_mi = 7; /* kernel.cl:844-870 ignores bc_type */
+        N.walls = s.bc_type == 1 ? 7 : 0;
+    } else {
+        N.periodic = s.periodic_mask & 7;
+        N.list_mi = N.periodic;
+        N.force_mi = N.periodic;
+        N.walls = (~N.periodic) & 7;
+    }
+    N.types_num = s.n_types;
+    return FN_OK;
+}
+
+void pair_coeffs(int kind, const double* raw, FnPair& P) {
+    std::memset(&P, 0, sizeof P);
+    P.kind = kind;
+    if (kind == FN_PAIR_LJ) {
+        P.c[0] = raw[0];
+        P.c[1] = raw[1];
+        P.c[2] = raw[2];
+        double r2 = P.c[2] * P.c[2];
+        double sigma2 = P.c[0];
+        double epsilon = P.c[1];
+        sigma2 *= sigma2;
+        double fr2 = sigma2 / r2;
+        double fr6 = fr2 * fr2 * fr2;
+        P.c[3] = 48.0 * epsilon * fr6 * (fr6 - 0.5) / r2;
+    } else if (kind == FN_PAIR_HS) {
+        P.c[0] = raw[0];
+    } else if (kind == FN_PAIR_ST) {
+        P.c[0] = raw[1];
+        P.c[1] = raw[2];
+        P.c[2] = raw[3] - P.c[1];
+        P.c[3] = raw[3] * raw[3];
+        P.c[4] = raw[0];
+        P.c[5] = 2 * raw[2] - raw[3];
+    }
+}
+
+double pack_w(float radius, int type) {
+    uint32_t lo;
+    std::memcpy(&lo, &radius, 4);
+    uint64_t bits = ((uint64_t)(uint32_t)type << 32) | lo;
+    double w;
+    std::memcpy(&w, &bits, 8);
+    return w;
+}
+
+int float_bits(float f) {
+    int b;
+    std::memcpy(&b, &f, 4);
+    return b;
+}
+
+/* Bead order inside one network: fibres (spring-connected components) sorted
+   by the Morton code of their first bead, beads of a fibre kept in file
+   order, so bonded partners stay adjacent and nearby fibres get nearby
+   indices. */
+void network_order(const fn_network_desc& d, const FnNet& N, bool reorder, std::vector<int>& order) {
+    const int n = d.n_beads;
+    order.resize(n);
+    std::iota(order.begin(), order.end(), 0);
+    if (!reorder || n == 0) return;
+    std::vector<int> parent(n);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int x) {
+        while (parent[x] != x) {
+            parent[x] = parent[parent[x]];
+            x = parent[x];
+        }
+        return x;
+    };
+    for (int s = 0; s < d.n_springs; ++s) {
+        int a = find(d.s_p1[s]), b = find(d.s_p2[s]);
+        if (a != b) parent[std::max(a, b)] = std::min(a, b);
+    }
+    std::vector<int> root(n);
+    for (int i = 0; i < n; ++i) root[i] = find(i);
+    std::vector<uint64_t> key(n);
+    for (int i = 0; i < n; ++i) {
+        if (root[i] != i) continue;
+        uint32_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            double x = d.pos[3 * i + a] / N.box[a] * 1024.0;
+            if (!(x >= 0.0)) x = 0.0;
+            if (x > 1023.0) x = 1023.0;
+            q[a] = (uint32_t)x;
+        }
+        uint64_t m = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
+        key[i] = (m << 32) | (uint32_t)i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        uint64_t ka = key[root[a]], kb = key[root[b]];
+        if (ka != kb) return ka < kb;
+        return a < b;
+    });
+}
+
+int build_tiles(fn_ctx* c, int block, std::vector<FnTile>& out) {
+    out.clear();
+    for (int k = 0; k < c->n_nets; ++k) {
+        const NetHost& h = c->info[k];
+        for (int b = h.bead_begin; b < h.bead_end; b += block) {
+            FnTile t;
+            t.net = k;
+            t.begin = b;
+            t.end = std::min(b + block, h.bead_end);
+            t.pad_ = 0;
+            out.push_back(t);
+        }
+    }
+    return (int)out.size();
+}
+
+int set_block(fn_ctx* c, int block) {
+    std::vector<FnTile> t;
+    int n = build_tiles(c, block, t);
+    CK(dalloc(c, c->tiles, t.size()));
+    CK(h2d(c, c->tiles, t));
+    c->ntiles = n;
+    c->block = block;
+    return FN_OK;
+}
+
+fn::StepArgs step_args(fn_ctx* c, bool pingpong) {
+    fn::StepArgs A{};
+    A.tiles = c->tiles.p;
+    A.nets = c->nets.p;
+    A.pairs = c->pairs.p;
+    A.pos_in = c->pos[c->cur].p;
+    A.img_in = c->img[c->cur].p;
+    A.pos_out = pingpong ? c->pos[1 - c->cur].p : c->pos[c->cur].p;
+    A.img_out = pingpong ? c->img[1 - c->cur].p : c->img[c->cur].p;
+    A.vold = c->vold.p;
+    A.force = c->force.p;
+    A.vel = c->vel.p;
+    A.sp_ends = c->sp_ends.p;
+    A.sp_par = c->sp_par.p;
+    A.sp_type = c->sp_type.p;
+    A.sp_status = c->sp_status.p;
+    A.an_b = c->an_b.p;
+    A.an_s = c->an_s.p;
+    A.an_par = c->an_par.p;
+    A.an_status = c->an_status.p;
+    A.sp_off = c->sp_off.p;
+    A.sp_ent = c->sp_ent.p;
+    A.an_off = c->an_off.p;
+    A.an_ent = c->an_ent.p;
+    A.list_count = c->list_count.p;
+    A.list = c->list.p;
+    A.list_stride = c->list_stride;
+    A.list_cap = c->cfg.list_capacity;
+    A.counters = c->counters.p;
+    return A;
+}
+
+fn::RebuildArgs rebuild_args(fn_ctx* c) {
+    fn::RebuildArgs R{};
+    R.tiles = c->tiles.p;
+    R.nets = c->nets.p;
+    R.pairs = c->pairs.p;
+    R.pos = c->pos[c->cur].p;
+    R.binfo = c->binfo.p;
+    R.cell_of = c->cell_of.p;
+    R.cell_count = c->cell_count.p;
+    R.cell_fill = c->cell_fill.p;
+    R.cell_start = c->cell_start.p;
+    R.cell_beads = c->cell_beads.p;
+    R.list_count = c->list_count.p;
+    R.list = c->list.p;
+    R.list_stride = c->list_stride;
+    R.list_cap = c->cfg.list_capacity;
+    R.cell_cap = c->cfg.cell_capacity;
+    R.counters = c->counters.p;
+    return R;
+}
+
+cudaEvent_t next_event(fn_ctx* c) {
+    if (c->ev_next >= c->ev_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_next++];
+}
+
+int do_rebuild(fn_ctx* c) {
+    fn::RebuildArgs R = rebuild_args(c);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->timing) {
+        e0 = next_event(c);
+        e1 = next_event(c);
+        CK(cudaEventRecord(e0, c->stream));
+    }
+    CK(fn::launch_rebuild(R, c->ntiles, c->block, (int)c->nb, c->ncells, c->scan_sums.p, c->stream));
+    if (c->timing) {
+        CK(cudaEventRecord(e1, c->stream));
+        c->ev_rebuild.emplace_back(e0, e1);
+    }
+    c->rebuilds_done++;
+    return FN_OK;
+}
+
+int launch_one_step(fn_ctx* c, bool do_drift, bool store_v) {
+    fn::StepArgs A = step_args(c, true);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->timing) {
+        e0 = next_event(c);
+        e1 = next_event(c);
+        CK(cudaEventRecord(e0, c->stream));
+    }
+    CK(fn::launch_step(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    if (c->timing) {
+        CK(cudaEventRecord(e1, c->stream));
+        c->ev_step.emplace_back(e0, e1);
+    }
+    if (do_drift) c->cur = 1 - c->cur;
+    return FN_OK;
+}
+
+int check_ready(fn_ctx* c) {
+    if (!c) return FN_ERR_ARG;
+    if (!c->uploaded) return fail(c, FN_ERR_STATE, "no model uploaded");
+    return FN_OK;
+}
+
+}  // namespace
+
+/* ======================================================================== */
+
+extern "C" {
+
+FN_API int fn_create(const fn_config* cfg, fn_ctx** out) {
+    if (!cfg || !out) return FN_ERR_ARG;
+    *out = nullptr;
+    fn_ctx* c = new fn_ctx();
+    c->cfg = *cfg;
+    if (c->cfg.cell_capacity <= 0) c->cfg.cell_capacity = 64;
+    if (c->cfg.list_capacity <= 0) c->cfg.list_capacity = 64;
+    if (c->cfg.block_size < 0 || c->cfg.block_size > 512 || (c->cfg.block_size % 32) != 0) {
+        delete c;
+        return FN_ERR_ARG;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) {
+        delete c;
+        return FN_ERR_CUDA;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) {
+        delete c;
+        return FN_ERR_ARG;
+    }
+    if (cudaSetDevice(cfg->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return FN_ERR_CUDA;
+    }
+    *out = c;
+    return FN_OK;
+}
+
+FN_API void fn_destroy(fn_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->cfg.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+FN_API const char* fn_last_error(const fn_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
+    if (!c || n_networks <= 0 || !nets) return fail(c, FN_ERR_ARG, "fn_upload: bad arguments");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    c->uploaded = false;
+    c->n_nets = n_networks;
+    c->nets_h.assign(n_networks, FnNet{});
+    c->info.assign(n_networks, NetHost{});
+    c->pairs_h.clear();
+    long long nb = 0, ns = 0, na = 0, ncells = 0;
+    c->damp = false;
+    for (int k = 0; k < n_networks; ++k) {
+        const fn_network_desc& d = nets[k];
+        if (d.n_beads <= 0 || d.n_springs < 0 || d.n_angles < 0)
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": empty or negative sizes");
+        if (!d.type || !d.tag || !d.loc_id || !d.radius || !d.mass || !d.pos || !d.vel ||
+            !d.vel_old || !d.force || !d.img || !d.pair_kind || !d.pair_raw)
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null bead array");
+        if (d.n_springs > 0 && (!d.s_type || !d.s_p1 || !d.s_p2 || !d.s_rest || !d.s_k || !d.s_c1 || !d.s_c2))
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null spring array");
+        if (d.n_angles > 0 && (!d.a_type || !d.a_b1 || !d.a_b2 || !d.a_b3 || !d.a_s1 || !d.a_s2 ||
+                               !d.a_theta0 || !d.a_k))
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null angle array");
+        int r = derive_net(c, d.settings, c->nets_h[k], k);
+        if (r) return r;
+        FnNet& N = c->nets_h[k];
+        const int nt = d.settings.n_types;
+        for (int i = 0; i < d.n_beads; ++i) {
+            if (d.type[i] < 0 || d.type[i] >= nt)
+                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": bead " +
+                                               std::to_string(i) + " has an undeclared type");
+            if (!(d.mass[i] >= 0.0))
+                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": negative mass");
+        }
+        for (int s = 0; s < d.n_springs; ++s)
+            if (d.s_p1[s] < 0 || d.s_p1[s] >= d.n_beads || d.s_p2[s] < 0 || d.s_p2[s] >= d.n_beads)
+                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": spring " +
+                                               std::to_string(s) + " references a missing bead");
+        for (int a = 0; a < d.n_angles; ++a) {
+            int b[3] = {d.a_b1[a], d.a_b2[a], d.a_b3[a]};
+            for (int q = 0; q < 3; ++q)
+                if (b[q] < 0 || b[q] >= d.n_beads)
+                    return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": angle " +
+                                                   std::to_string(a) + " references a missing bead");
+            if (d.a_type[a] == 1 && (d.a_s1[a] < 0 || d.a_s1[a] >= d.n_springs || d.a_s2[a] < 0 ||
+                                     d.a_s2[a] >= d.n_springs))
+                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": HR_FL angle " +
+                                               std::to_string(a) + " references a missing spring");
+        }
+        const int npairs = nt * (nt + 1) / 2;
+        N.pair_base = (int)c->pairs_h.size();
+        for (int p = 0; p < npairs; ++p) {
+            FnPair P;
+            pair_coeffs(d.pair_kind[p], d.pair_raw + 4 * p, P);
+            c->pairs_h.push_back(P);
+        }
+        NetHost& h = c->info[k];
+        h.bead_begin = (int)nb;
+        h.bead_end = (int)(nb + d.n_beads);
+        h.spring_begin = (int)ns;
+        h.spring_end = (int)(ns + d.n_springs);
+        h.angle_begin = (int)na;
+        h.angle_end = (int)(na + d.n_angles);
+        h.cell_begin = ncells;
+        h.cell_end = ncells + (long long)N.nx * N.ny * N.nz;
+        h.grid_update_freq = d.settings.grid_update_freq;
+        h.damping = N.damping;
+        N.cell_base = (int)ncells;
+        N.bead_begin = h.bead_begin;
+        N.bead_end = h.bead_end;
+        if (N.damping != 0.0) c->damp = true;
+        if (h.grid_update_freq <= 0) return fail(c, FN_ERR_ARG, "grid_update_freq must be positive");
+        if (k > 0 && h.grid_update_freq != c->info[0].grid_update_freq)
+            return fail(c, FN_ERR_UNSUPPORTED, "all networks of a batch must share grid_update_freq");
+        nb += d.n_beads;
+        ns += d.n_springs;
+        na += d.n_angles;
+        ncells = h.cell_end;
+        if (nb > 0x7fffffffLL || ns > 0x3fffffffLL || na > 0x1fffffffLL || ncells > 0x7fffffffLL)
+            return fail(c, FN_ERR_ARG, "model too large for 32-bit indices");
+    }
+    c->nb = nb;
+    c->ns = ns;
+    c->na = na;
+    c->ncells = ncells;
+    c->grid_update_freq = c->info[0].grid_update_freq;
+
+    /* bead order */
+    c->perm.assign(nb, 0);
+    c->inv.assign(nb, 0);
+    for (int k = 0; k < n_networks; ++k) {
+        std::vector<int> order;
+        network_order(nets[k], c->nets_h[k], c->cfg.reorder != 0, order);
+        const int base = c->info[k].bead_begin;
+        for (int q = 0; q < (int)order.size(); ++q) {
+            c->perm[base + q] = base + order[q];
+            c->inv[base + order[q]] = base + q;
+        }
+    }
+
+    /* bead arrays in internal order */
+    std::vector<double4> pos(nb), img(nb);
+    std::vector<float4> vold(nb), force(nb), vel(nb);
+    std::vector<int4> binfo(nb);
+    c->mass_h.assign(nb, 0.0);
+    c->radius_h.assign(nb, 0.0);
+    for (int k = 0; k < n_networks; ++k) {
+        const fn_network_desc& d = nets[k];
+        const int base = c->info[k].bead_begin;
+        for (int i = 0; i < d.n_beads; ++i) {
+            const int q = c->inv[base + i];
+            const float rad = (float)d.radius[i];
+            const double mass = d.mass[i];
+            const double minv = mass > 0.0 ? 1.0 / mass : 0.0; /* SimulationManager.cpp:1435-1445 */
+            c->mass_h[base + i] = mass;
+            c->radius_h[base + i] = d.radius[i];
+            pos[q] = make_double4(d.pos[3 * i], d.pos[3 * i + 1], d.pos[3 * i + 2], pack_w(rad, d.type[i]));
+            img[q] = make_double4(d.img[3 * i], d.img[3 * i + 1], d.img[3 * i + 2], minv);
+            vold[q] = make_float4((float)d.vel_old[3 * i], (float)d.vel_old[3 * i + 1],
+                                  (float)d.vel_old[3 * i + 2], 0.f);
+            force[q] = make_float4((float)d.force[3 * i], (float)d.force[3 * i + 1],
+                                   (float)d.force[3 * i + 2], 0.f);
+            vel[q] = make_float4((float)d.vel[3 * i], (float)d.vel[3 * i + 1], (float)d.vel[3 * i + 2], 0.f);
+            const float skin = (float)((double)rad + d.settings.skin_ratio);
+            binfo[q] = make_int4(d.tag[i], d.loc_id[i], d.type[i], float_bits(skin));
+        }
+    }
+
+    /* springs and angles keep their (concatenated) file order */
+    std::vector<int2> sp_ends(ns);
+    std::vector<signed char> sp_type(ns), sp_status(ns, 1);
+    c->sp_par_h.assign(ns, make_float4(0, 0, 0, 0));
+    std::vector<int4> an_b(na);
+    std::vector<int2> an_s(na);
+    std::vector<signed char> an_status(na, 1);
+    c->an_par_h.assign(na, make_float2(0, 0));
+    for (int k = 0; k < n_networks; ++k) {
+        const fn_network_desc& d = nets[k];
+        const NetHost& h = c->info[k];
+        for (int s = 0; s < d.n_springs; ++s) {
+            const int g = h.spring_begin + s;
+            sp_ends[g] = make_int2(c->inv[h.bead_begin + d.s_p1[s]], c->inv[h.bead_begin + d.s_p2[s]]);
+            sp_type[g] = (signed char)d.s_type[s];
+            c->sp_par_h[g] = make_float4((float)d.s_rest[s], (float)d.s_k[s], (float)d.s_c1[s], (float)d.s_c2[s]);
+        }
+        for (int a = 0; a < d.n_angles; ++a) {
+            const int g = h.angle_begin + a;
+            an_b[g] = make_int4(c->inv[h.bead_begin + d.a_b1[a]], c->inv[h.bead_begin + d.a_b2[a]],
+                                c->inv[h.bead_begin + d.a_b3[a]], d.a_type[a]);
+            const int s1 = d.a_type[a] == 1 ? h.spring_begin + d.a_s1[a] : 0;
+            const int s2 = d.a_type[a] == 1 ? h.spring_begin + d.a_s2[a] : 0;
+            an_s[g] = make_int2(s1, s2);
+            c->an_par_h[g] = make_float2((float)d.a_theta0[a], (float)d.a_k[a]);
+        }
+    }
+
+    /* bead -> bond incidence, ascending bond index per bead */
+    std::vector<int> sp_off(nb + 1, 0), an_off(nb + 1, 0);
+    for (long long s = 0; s < ns; ++s) {
+        sp_off[sp_ends[s].x + 1]++;
+        sp_off[sp_ends[s].y + 1]++;
+    }
+    for (long long a = 0; a < na; ++a) {
+        an_off[an_b[a].x + 1]++;
+        an_off[an_b[a].y + 1]++;
+        an_off[an_b[a].z + 1]++;
+    }
+    for (long long i = 0; i < nb; ++i) {
+        sp_off[i + 1] += sp_off[i];
+        an_off[i + 1] += an_off[i];
+    }
+    std::vector<int> sp_ent(2 * ns), an_ent(3 * na);
+    {
+        std::vector<int> fill(sp_off.begin(), sp_off.end() - 1);
+        for (long long s = 0; s < ns; ++s) {
+            sp_ent[fill[sp_ends[s].x]++] = (int)(s << 1);
+            sp_ent[fill[sp_ends[s].y]++] = (int)((s << 1) | 1);
+        }
+        std::vector<int> fa(an_off.begin(), an_off.end() - 1);
+        for (long long a = 0; a < na; ++a) {
+            an_ent[fa[an_b[a].x]++] = (int)(a << 2);
+            an_ent[fa[an_b[a].y]++] = (int)((a << 2) | 1);
+            an_ent[fa[an_b[a].z]++] = (int)((a << 2) | 2);
+        }
+    }
+
+    c->list_stride = (int)((nb + 31) / 32 * 32);
+    const size_t list_n = (size_t)c->list_stride * (size_t)c->cfg.list_capacity;
+    for (int k = 0; k < 2; ++k) {
+        CK(dalloc(c, c->pos[k], nb));
+        CK(dalloc(c, c->img[k], nb));
+    }
+    CK(dalloc(c, c->vold, nb));
+    CK(dalloc(c, c->force, nb));
+    CK(dalloc(c, c->vel, nb));
+    CK(dalloc(c, c->binfo, nb));
+    CK(dalloc(c, c->sp_ends, ns));
+    CK(dalloc(c, c->sp_par, ns));
+    CK(dalloc(c, c->sp_type, ns));
+    CK(dalloc(c, c->sp_status, ns));
+    CK(dalloc(c, c->an_b, na));
+    CK(dalloc(c, c->an_s, na));
+    CK(dalloc(c, c->an_par, na));
+    CK(dalloc(c, c->an_status, na));
+    CK(dalloc(c, c->sp_off, nb + 1));
+    CK(dalloc(c, c->sp_ent, 2 * ns));
+    CK(dalloc(c, c->an_off, nb + 1));
+    CK(dalloc(c, c->an_ent, 3 * na));
+    CK(dalloc(c, c->cell_of, nb));
+    CK(dalloc(c, c->cell_count, ncells));
+    CK(dalloc(c, c->cell_fill, ncells));
+    CK(dalloc(c, c->cell_start, ncells + 1));
+    CK(dalloc(c, c->cell_beads, nb));
+    CK(dalloc(c, c->list_count, nb));
+    CK(dalloc(c, c->list, list_n));
+    CK(dalloc(c, c->scan_sums, (size_t)fn::scan_block_count(ncells) + 1));
+    CK(dalloc(c, c->nets, n_networks));
+    CK(dalloc(c, c->pairs, c->pairs_h.size()));
+    CK(dalloc(c, c->counters, FN_CNT_N));
+    CK(dalloc(c, c->obs_partial, 5 * 1024));
+    CK(dalloc(c, c->obs_out, 8));
+
+    c->cur = 0;
+    CK(h2d(c, c->pos[0], pos));
+    CK(h2d(c, c->img[0], img));
+    CK(h2d(c, c->pos[1], pos));
+    CK(h2d(c, c->img[1], img));
+    CK(h2d(c, c->vold, vold));
+    CK(h2d(c, c->force, force));
+    CK(h2d(c, c->vel, vel));
+    CK(h2d(c, c->binfo, binfo));
+    CK(h2d(c, c->sp_ends, sp_ends));
+    CK(h2d(c, c->sp_par, c->sp_par_h));
+    CK(h2d(c, c->sp_type, sp_type));
+    CK(h2d(c, c->sp_status, sp_status));
+    CK(h2d(c, c->an_b, an_b));
+    CK(h2d(c, c->an_s, an_s));
+    CK(h2d(c, c->an_par, c->an_par_h));
+    CK(h2d(c, c->an_status, an_status));
+    CK(h2d(c, c->sp_off, sp_off));
+    CK(h2d(c, c->sp_ent, sp_ent));
+    CK(h2d(c, c->an_off, an_off));
+    CK(h2d(c, c->an_ent, an_ent));
+    CK(h2d(c, c->nets, c->nets_h));
+    CK(h2d(c, c->pairs, c->pairs_h));
+    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * FN_CNT_N, c->stream));
+    CK(cudaMemsetAsync(c->list_count.p, 0, sizeof(int) * (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
+    int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128);
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    c->steps_done = 0;
+    c->rebuilds_done = 0;
+    c->uploaded = true;
+    return FN_OK;
+}
+
+FN_API int fn_step(fn_ctx* c, int nsteps) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (nsteps <= 0) return fail(c, FN_ERR_ARG, "RunSimulationLoop: loop size should be a positive number");
+    CK(cudaSetDevice(c->cfg.device));
+    /* AdvancePosition of step 0 */
+    {
+        fn::StepArgs A = step_args(c, false);
+        CK(fn::launch_drift(A, c->ntiles, c->block, c->damp || nsteps == 1, c->stream));
+    }
+    int grid_update_cnt = 0; /* local, as SimulationManager.cpp:152 */
+    for (int step = 0; step < nsteps; ++step) {
+        if (grid_update_cnt == c->grid_update_freq) grid_update_cnt = 0;
+        if (grid_update_cnt == 0) {
+            r = do_rebuild(c);
+            if (r) return r;
+        }
+        const bool last = step == nsteps - 1;
+        r = launch_one_step(c, !last, step == nsteps - 2);
+        if (r) return r;
+        grid_update_cnt++;
+    }
+    c->steps_done += nsteps;
+    return FN_OK;
+}
+
+FN_API int fn_rebuild_contacts(fn_ctx* c) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    return do_rebuild(c);
+}
+
+FN_API int fn_reset_energy(fn_ctx* c) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(fn::launch_reset_energy(c->force.p, c->vel.p, c->vold.p, (int)c->nb, c->stream));
+    return FN_OK;
+}
+
+FN_API int fn_sync(fn_ctx* c) {
+    if (!c) return FN_ERR_ARG;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    return FN_OK;
+}
+
+FN_API int fn_download(fn_ctx* c, int field, double* host) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!host) return fail(c, FN_ERR_ARG, "fn_download: null host pointer");
+    CK(cudaSetDevice(c->cfg.device));
+    const long long nb = c->nb;
+    if (field == FN_POSITION || field == FN_IMAGE) {
+        std::vector<double4> tmp(nb);
+        const DevBuf<double4>& b = field == FN_POSITION ? c->pos[c->cur] : c->img[c->cur];
+        CK(cudaMemcpyAsync(tmp.data(), b.p, sizeof(double4) * nb, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (long long q = 0; q < nb; ++q) {
+            const long long i = c->perm[q];
+            host[3 * i] = tmp[q].x;
+            host[3 * i + 1] = tmp[q].y;
+            host[3 * i + 2] = tmp[q].z;
+        }
+        return FN_OK;
+    }
+    const DevBuf<float4>* b = field == FN_VELOCITY ? &c->vel
+                              : field == FN_FORCE  ? &c->force
+                              : field == FN_VELOCITY_OLD ? &c->vold
+                                                         : nullptr;
+    if (!b) return fail(c, FN_ERR_ARG, "fn_download: unknown field");
+    std::vector<float4> tmp(nb);
+    CK(cudaMemcpyAsync(tmp.data(), b->p, sizeof(float4) * nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (long long q = 0; q < nb; ++q) {
+        const long long i = c->perm[q];
+        host[3 * i] = tmp[q].x;
+        host[3 * i + 1] = tmp[q].y;
+        host[3 * i + 2] = tmp[q].z;
+    }
+    return FN_OK;
+}
+
+FN_API int fn_set_beads(fn_ctx* c, int field, const double* host) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!host) return fail(c, FN_ERR_ARG, "fn_set_beads: null host pointer");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    const long long nb = c->nb;
+    if (field == FN_POSITION || field == FN_IMAGE) {
+        DevBuf<double4>& b = field == FN_POSITION ? c->pos[c->cur] : c->img[c->cur];
+        std::vector<double4> tmp(nb);
+        CK(cudaMemcpy(tmp.data(), b.p, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
+        for (long long q = 0; q < nb; ++q) {
+            const long long i = c->perm[q];
+            tmp[q].x = host[3 * i];
+            tmp[q].y = host[3 * i + 1];
+            tmp[q].z = host[3 * i + 2];
+        }
+        CK(cudaMemcpy(b.p, tmp.data(), sizeof(double4) * nb, cudaMemcpyHostToDevice));
+        return FN_OK;
+    }
+    DevBuf<float4>* b = field == FN_VELOCITY ? &c->vel
+                        : field == FN_FORCE  ? &c->force
+                        : field == FN_VELOCITY_OLD ? &c->vold
+                                                   : nullptr;
+    if (!b) return fail(c, FN_ERR_ARG, "fn_set_beads: unknown field");
+    std::vector<float4> tmp(nb);
+    for (long long q = 0; q < nb; ++q) {
+        const long long i = c->perm[q];
+        tmp[q] = make_float4((float)host[3 * i], (float)host[3 * i + 1], (float)host[3 * i + 2], 0.f);
+    }
+    CK(cudaMemcpy(b->p, tmp.data(), sizeof(float4) * nb, cudaMemcpyHostToDevice));
+    return FN_OK;
+}
+
+FN_API int fn_set_mass(fn_ctx* c, const double* mass) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!mass) return fail(c, FN_ERR_ARG, "fn_set_mass: null pointer");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    const long long nb = c->nb;
+    for (long long i = 0; i < nb; ++i)
+        if (!(mass[i] >= 0.0)) return fail(c, FN_ERR_ARG, "fn_set_mass: mass must be zero or positive");
+    std::vector<double4> tmp(nb);
+    CK(cudaMemcpy(tmp.data(), c->img[c->cur].p, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
+    for (long long q = 0; q < nb; ++q) {
+        const double m = mass[c->perm[q]];
+        tmp[q].w = m > 0.0 ? 1.0 / m : 0.0;
+        c->mass_h[c->perm[q]] = m;
+    }
+    CK(cudaMemcpy(c->img[c->cur].p, tmp.data(), sizeof(double4) * nb, cudaMemcpyHostToDevice));
+    return FN_OK;
+}
+
+FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!skin) return fail(c, FN_ERR_ARG, "fn_set_skin: null pointer");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    const long long nb = c->nb;
+    std::vector<int4> tmp(nb);
+    CK(cudaMemcpy(tmp.data(), c->binfo.p, sizeof(int4) * nb, cudaMemcpyDeviceToHost));
+    for (long long q = 0; q < nb; ++q) tmp[q].w = float_bits((float)skin[c->perm[q]]);
+    CK(cudaMemcpy(c->binfo.p, tmp.data(), sizeof(int4) * nb, cudaMemcpyHostToDevice));
+    return FN_OK;
+}
+
+FN_API int fn_set_springs(fn_ctx* c, const double* rest, const double* k, const double* c1,
+                          const double* c2) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    for (long long s = 0; s < c->ns; ++s) {
+        float4& p = c->sp_par_h[s];
+        if (rest) p.x = (float)rest[s];
+        if (k) p.y = (float)k[s];
+        if (c1) p.z = (float)c1[s];
+        if (c2) p.w = (float)c2[s];
+    }
+    if (c->ns > 0)
+        CK(cudaMemcpy(c->sp_par.p, c->sp_par_h.data(), sizeof(float4) * c->ns, cudaMemcpyHostToDevice));
+    return FN_OK;
+}
+
+FN_API int fn_set_angles(fn_ctx* c, const double* theta0, const double* k) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    for (long long a = 0; a < c->na; ++a) {
+        if (theta0) c->an_par_h[a].x = (float)theta0[a];
+        if (k) c->an_par_h[a].y = (float)k[a];
+    }
+    if (c->na > 0)
+        CK(cudaMemcpy(c->an_par.p, c->an_par_h.data(), sizeof(float2) * c->na, cudaMemcpyHostToDevice));
+    return FN_OK;
+}
+
+FN_API int fn_download_status(fn_ctx* c, int* spring_status, int* angle_status) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    std::vector<signed char> s(c->ns), a(c->na);
+    if (c->ns > 0 && spring_status)
+        CK(cudaMemcpyAsync(s.data(), c->sp_status.p, c->ns, cudaMemcpyDeviceToHost, c->stream));
+    if (c->na > 0 && angle_status)
+        CK(cudaMemcpyAsync(a.data(), c->an_status.p, c->na, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (spring_status)
+        for (long long q = 0; q < c->ns; ++q) spring_status[q] = s[q];
+    if (angle_status)
+        for (long long q = 0; q < c->na; ++q) angle_status[q] = a[q];
+    return FN_OK;
+}
+
+FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_status) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (spring_status && c->ns > 0) {
+        std::vector<signed char> s(c->ns);
+        for (long long q = 0; q < c->ns; ++q) s[q] = (signed char)spring_status[q];
+        CK(cudaMemcpy(c->sp_status.p, s.data(), c->ns, cudaMemcpyHostToDevice));
+    }
+    if (angle_status && c->na > 0) {
+        std::vector<signed char> a(c->na);
+        for (long long q = 0; q < c->na; ++q) a[q] = (signed char)angle_status[q];
+        CK(cudaMemcpy(c->an_status.p, a.data(), c->na, cudaMemcpyHostToDevice));
+    }
+    return FN_OK;
+}
+
+FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_observe: bad arguments");
+    CK(cudaSetDevice(c->cfg.device));
+    const NetHost& h = c->info[net];
+    fn::ObserveArgs O{};
+    O.pos = c->pos[c->cur].p;
+    O.force = c->force.p;
+    O.sp_status = c->sp_status.p;
+    O.an_status = c->an_status.p;
+    O.bead_begin = h.bead_begin;
+    O.bead_end = h.bead_end;
+    O.spring_begin = h.spring_begin;
+    O.spring_end = h.spring_end;
+    O.angle_begin = h.angle_begin;
+    O.angle_end = h.angle_end;
+    O.reaction_type = reaction_type;
+    O.partial = c->obs_partial.p;
+    long long span = std::max({(long long)(h.bead_end - h.bead_begin), (long long)(h.spring_end - h.spring_begin),
+                               (long long)(h.angle_end - h.angle_begin), 1LL});
+    int nblocks = (int)std::min<long long>(1024, (span + 255) / 256);
+    CK(fn::launch_observe(O, nblocks, c->obs_out.p, c->stream));
+    double res[5];
+    CK(cudaMemcpyAsync(res, c->obs_out.p, sizeof res, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int a = 0; a < 3; ++a) out->reaction[a] = res[a];
+    out->broken = (long long)res[3];
+    out->angles_dead = (long long)res[4];
+    return FN_OK;
+}
+
+FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
+    if (!c || !out) return FN_ERR_ARG;
+    std::memset(out, 0, sizeof *out);
+    out->block_size = c->block;
+    out->n_networks = c->n_nets;
+    out->n_beads = c->nb;
+    out->device_bytes = c->device_bytes;
+    out->steps = c->steps_done;
+    out->rebuilds = c->rebuilds_done;
+    if (!c->uploaded) return FN_OK;
+    CK(cudaSetDevice(c->cfg.device));
+    unsigned long long cnt[FN_CNT_N];
+    CK(cudaMemcpyAsync(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->cell_overflow = (long long)cnt[FN_CNT_CELL_OVERFLOW];
+    out->list_overflow = (long long)cnt[FN_CNT_LIST_OVERFLOW];
+    if (cnt[FN_CNT_NONFINITE]) c->err = "non-finite force detected";
+    return FN_OK;
+}
+
+FN_API long long fn_n_cells(fn_ctx* c) { return c ? c->ncells : -1; }
+
+FN_API int fn_get_cells(fn_ctx* c, int* bead_cell, int* cell_count, long long n_cells) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    if (bead_cell) {
+        std::vector<int> tmp(c->nb);
+        CK(cudaMemcpyAsync(tmp.data(), c->cell_of.p, sizeof(int) * c->nb, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (long long q = 0; q < c->nb; ++q) bead_cell[c->perm[q]] = tmp[q];
+    }
+    if (cell_count) {
+        if (n_cells != c->ncells) return fail(c, FN_ERR_ARG, "fn_get_cells: wrong cell count");
+        CK(cudaMemcpyAsync(cell_count, c->cell_count.p, sizeof(int) * c->ncells, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return FN_OK;
+}
+
+FN_API int fn_get_lists(fn_ctx* c, int* count, int* partners, int cap) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    const long long nb = c->nb;
+    std::vector<int> cnt(nb);
+    CK(cudaMemcpyAsync(cnt.data(), c->list_count.p, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream));
+    std::vector<int> lst;
+    if (partners) {
+        lst.resize((size_t)c->list_stride * c->cfg.list_capacity);
+        CK(cudaMemcpyAsync(lst.data(), c->list.p, sizeof(int) * lst.size(), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    for (long long q = 0; q < nb; ++q) {
+        const long long i = c->perm[q];
+        if (count) count[i] = cnt[q];
+        if (partners) {
+            const int n = std::min(std::min(cnt[q], c->cfg.list_capacity), cap);
+            for (int k = 0; k < n; ++k)
+                partners[(size_t)i * cap + k] = c->perm[lst[(size_t)k * c->list_stride + q]];
+        }
+    }
+    return FN_OK;
+}
+
+FN_API int fn_get_permutation(fn_ctx* c, int* perm) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!perm) return FN_ERR_ARG;
+    std::memcpy(perm, c->perm.data(), sizeof(int) * c->nb);
+    return FN_OK;
+}
+
+/* Starts (on != 0) or stops a timing window: while on, every step-kernel
+   launch and every rebuild is bracketed by CUDA events on the context's
+   stream; fn_kernel_time averages the window. */
+FN_API int fn_enable_timing(fn_ctx* c, int on) {
+    if (!c) return FN_ERR_ARG;
+    if (on) {
+        CK(cudaSetDevice(c->cfg.device));
+        CK(cudaStreamSynchronize(c->stream));
+        c->ev_next = 0;
+        c->ev_step.clear();
+        c->ev_rebuild.clear();
+    }
+    c->timing = on != 0;
+    return FN_OK;
+}
+
+FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, double* rebuild_ms,
+                          long long* rebuilds) {
+    if (!c) return FN_ERR_ARG;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    double ts = 0.0, tr = 0.0;
+    for (auto& p : c->ev_step) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, p.first, p.second));
+        ts += ms;
+    }
+    for (auto& p : c->ev_rebuild) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, p.first, p.second));
+        tr += ms;
+    }
+    if (step_ms) *step_ms = c->ev_step.empty() ? 0.0 : ts / (double)c->ev_step.size();
+    if (launches) *launches = (long long)c->ev_step.size();
+    if (rebuild_ms) *rebuild_ms = c->ev_rebuild.empty() ? 0.0 : tr / (double)c->ev_rebuild.size();
+    if (rebuilds) *rebuilds = (long long)c->ev_rebuild.size();
+    return FN_OK;
+}
+
+FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
+    return fail(c, FN_ERR_UNSUPPORTED, "autotune not built yet");
+}
+
+/* Forces alone at the current positions (zeroed, no base term), for the
+   one-step parity checks: terms bit 0 springs, 1 angles, 2 contacts. */
+FN_API int fn_forces_only(fn_ctx* c, int terms) {
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    fn::StepArgs A = step_args(c, false);
+    CK(fn::launch_forces_only(A, c->ntiles, c->block, terms, c->stream));
+    return FN_OK;
+}
+
+}  // extern "C"

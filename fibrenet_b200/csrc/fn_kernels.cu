@@ -1,0 +1,806 @@
+/*
+ * fn_kernels.cu -- sm_100a kernels of the FibreNet step loop.
+ *
+ * One time step is one launch of k_step: every thread owns one bead and
+ *   1. rebuilds the base force the reference writes in AdvancePosition
+ *      (damping * v + gravity + wall penalty, kernel.cl:231-261),
+ *   2. gathers its incident springs (kernel.cl:366-441), angles
+ *      (kernel.cl:268-363) and contacts (kernel.cl:792-1011) in a fixed order
+ *      instead of the reference's FP64 atomics,
+ *   3. applies AdvanceVelocity (kernel.cl:444-464), and
+ *   4. applies the next step's AdvancePosition (kernel.cl:195-265), writing the
+ *      drifted position into the other half of a ping-pong pair so neighbours
+ *      still read this step's positions.
+ * A standalone k_drift opens each fn_step call.  The contact list is rebuilt
+ * between steps (k_cells -> scan -> k_scatter -> k_cell_sort -> k_lists),
+ * giving the same pair set as FillGrid + BuildContactList (kernel.cl:487-789)
+ * with deterministic order.
+ *
+ * All force arithmetic is FP64 with the reference's operation order; the
+ * library is built with -fmad=false so nothing is contracted into FMAs, which
+ * keeps results bit-identical to the host mirror checker.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fn_detmath.h"
+#include "fn_kernels.h"
+#include "fn_types.h"
+
+namespace fn {
+
+__device__ __forceinline__ float w_radius(double w) { return __int_as_float(__double2loint(w)); }
+__device__ __forceinline__ int w_type(double w) { return __double2hiint(w); }
+
+/* GETADRESS, kernel.cl:9 */
+__device__ __forceinline__ int getadress(int t1, int t2, int size) {
+    return (t1 < t2) ? ((size * t1) + t2 - ((t1 * (t1 + 1)) / 2))
+                     : ((size * t2) + t1 - ((t2 * (t2 + 1)) / 2));
+}
+
+/* Spring s (kernel.cl:371-437): returns 1 when a force acts, f = force on p1
+   (p2 takes f * -1.0); broke = 1 when this evaluation breaks an HR_FL
+   spring (kernel.cl:391-397). */
+__device__ __forceinline__ int spring_eval(const StepArgs& A, int s, double& fx, double& fy,
+                                           double& fz, int& broke) {
+    broke = 0;
+    const int type = A.sp_type[s];
+    if (!(type == 0 || type == 1)) return 0;
+    if (A.sp_status[s] != 1) return 0;
+    const int2 e = A.sp_ends[s];
+    const double4 a = A.img_in[e.x];
+    const double4 b = A.img_in[e.y];
+    const float4 par = A.sp_par[s];
+    double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    double l = sqrt(dx * dx + dy * dy + dz * dz);
+    double factor = (double)par.x - l;
+    if (l != 0.0) l = 1.0 / l;
+    dx *= l;
+    dy *= l;
+    dz *= l;
+    if (type == 1) {
+        double stress = -(double)par.z * factor * l;
+        if (fabs(stress) > (double)par.w) {
+            broke = 1;
+            return 0;
+        }
+    }
+    factor *= (double)par.y;
+    fx = dx * factor;
+    fy = dy * factor;
+    fz = dz * factor;
+    return 1;
+}
+
+__device__ __forceinline__ int spring_alive_after(const StepArgs& A, int s) {
+    if (A.sp_status[s] != 1) return 0;
+    double fx, fy, fz;
+    int broke;
+    spring_eval(A, s, fx, fy, fz, broke);
+    return !broke;
+}
+
+/* Angle force (kernel.cl:291-348): pa acts on b1, pc on b3. */
+__device__ __forceinline__ void angle_eval(const StepArgs& A, int4 b, float2 par, double& pax,
+                                           double& pay, double& paz, double& pcx, double& pcy,
+                                           double& pcz) {
+    const double4 t2 = A.img_in[b.y];
+    const double4 t1 = A.img_in[b.x];
+    const double4 t3 = A.img_in[b.z];
+    const double bax = t1.x - t2.x, bay = t1.y - t2.y, baz = t1.z - t2.z;
+    const double bcx = t3.x - t2.x, bcy = t3.y - t2.y, bcz = t3.z - t2.z;
+    const double cbx = bcx * -1.0, cby = bcy * -1.0, cbz = bcz * -1.0;
+    const double l_ba = sqrt(bax * bax + bay * bay + baz * baz);
+    const double l_bc = sqrt(bcx * bcx + bcy * bcy + bcz * bcz);
+    double dotp = (bax * bcx + bay * bcy + baz * bcz) / (l_ba * l_bc);
+    if (dotp < -1.0) dotp = -0.999999;
+    if (dotp > 1.0) dotp = 0.999999;
+    const double angle = fn_acos(dotp);
+    const double magnitude = -2.0 * (double)par.y * (angle - (double)par.x);
+    const double fa = magnitude / l_ba;
+    const double fc = magnitude / l_bc;
+    const double tx = bay * bcz - baz * bcy;
+    const double ty = baz * bcx - bax * bcz;
+    const double tz = bax * bcy - bay * bcx;
+    pax = (bay * tz - baz * ty);
+    pay = (baz * tx - bax * tz);
+    paz = (bax * ty - bay * tx);
+    double ln = sqrt(pax * pax + pay * pay + paz * paz);
+    if (ln != 0.0) ln = 1.0 / ln;
+    ln *= fa;
+    pax *= ln;
+    pay *= ln;
+    paz *= ln;
+    pcx = (cby * tz - cbz * ty);
+    pcy = (cbz * tx - cbx * tz);
+    pcz = (cbx * ty - cby * tx);
+    ln = sqrt(pcx * pcx + pcy * pcy + pcz * pcz);
+    if (ln != 0.0) ln = 1.0 / ln;
+    ln *= fc;
+    pcx *= ln;
+    pcy *= ln;
+    pcz *= ln;
+}
+
+/* Minimum image on the axes of mask (kernel.cl:598-627, 844-870). */
+__device__ __forceinline__ double min_image(const FnNet& N, double& rx, double& ry, double& rz,
+                                            double length, int mask) {
+    const double maxDim = N.half_box_sq;
+    if (length > maxDim) {
+        if ((mask & 1) && rx * rx > maxDim) rx = rx > 0.0 ? rx - N.box[0] : rx + N.box[0];
+        if ((mask & 2) && ry * ry > maxDim) ry = ry > 0.0 ? ry - N.box[1] : ry + N.box[1];
+        if ((mask & 4) && rz * rz > maxDim) rz = rz > 0.0 ? rz - N.box[2] : rz + N.box[2];
+        length = rx * rx + ry * ry + rz * rz;
+    }
+    return length;
+}
+
+/* One contact-list entry (kernel.cl:835-999): force on bead i. */
+__device__ __forceinline__ int contact_eval(const FnNet& N, const FnPair* __restrict__ pairs,
+                                            double4 pi, double4 pj, double& Rx, double& Ry,
+                                            double& Rz) {
+    double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+    double length = rx * rx + ry * ry + rz * rz;
+    length = min_image(N, rx, ry, rz, length, N.force_mi);
+    const int pid = N.pair_base + getadress(w_type(pi.w), w_type(pj.w), N.types_num);
+    const FnPair* P = pairs + pid;
+    const int kind = P->kind;
+    if (kind == 1) {
+        if (length < N.cutoff_sq) {
+            const double r2 = length;
+            length = sqrt(length);
+            if (length < P->c[2]) {
+                double sigma2 = P->c[0];
+                const double epsilon = P->c[1];
+                sigma2 *= sigma2;
+                const double fr2 = sigma2 / r2;
+                const double fr6 = fr2 * fr2 * fr2;
+                double fpr = 48.0 * epsilon * fr6 * (fr6 - 0.5) / r2;
+                fpr -= P->c[3];
+                length = (length != 0.0) ? 1.0 / length : 0.0;
+                Rx = fpr * (rx * length);
+                Ry = fpr * (ry * length);
+                Rz = fpr * (rz * length);
+                return 1;
+            }
+        }
+        return 0;
+    }
+    if (kind == 2) {
+        length = sqrt(length);
+        const double K = P->c[0];
+        double penetration = ((double)w_radius(pi.w) + (double)w_radius(pj.w)) - length;
+        if (penetration > 0.0) {
+            length = (length != 0.0) ? 1.0 / length : 0.0;
+            penetration *= K;
+            Rx = penetration * (rx * length);
+            Ry = penetration * (ry * length);
+            Rz = penetration * (rz * length);
+            return 1;
+        }
+        return 0;
+    }
+    if (kind == 3) {
+        if (length < P->c[3]) {
+            length = sqrt(length);
+            double factor = (P->c[1] - length);
+            factor *= P->c[0]; /* both arms of kernel.cl:970-973 multiply by K */
+            factor += (P->c[5] - length) * P->c[4];
+            length = (length != 0.0) ? 1.0 / length : 0.0;
+            Rx = factor * (rx * length);
+            Ry = factor * (ry * length);
+            Rz = factor * (rz * length);
+            return 1;
+        }
+        return 0;
+    }
+    return 0;
+}
+
+/* AdvancePosition (kernel.cl:200-250) on registers: returns the drifted
+   position/image, the predicted velocity. */
+__device__ __forceinline__ void drift(const FnNet& N, double minv, float fx, float fy, float fz,
+                                      float vox, float voy, float voz, double4& p, double4& im,
+                                      float4& v) {
+    const double lambda_dt = N.lambda_dt * minv;
+    const double half_dt2 = N.half_dt2 * minv;
+    v.x = (float)((double)fx * lambda_dt + (double)vox);
+    v.y = (float)((double)fy * lambda_dt + (double)voy);
+    v.z = (float)((double)fz * lambda_dt + (double)voz);
+    v.w = 0.0f;
+    double ix = (double)vox, iy = (double)voy, iz = (double)voz;
+    ix *= N.dt;
+    iy *= N.dt;
+    iz *= N.dt;
+    ix = (double)fx * half_dt2 + ix;
+    iy = (double)fy * half_dt2 + iy;
+    iz = (double)fz * half_dt2 + iz;
+    p.x += ix;
+    p.y += iy;
+    p.z += iz;
+    im.x += ix;
+    im.y += iy;
+    im.z += iz;
+    /* snap wrap, kernel.cl:241-250 */
+    if (N.periodic & 4)
+        if (p.z < 0.0) p.z = N.box[2];
+    if (N.periodic & 2)
+        if (p.y < 0.0) p.y = N.box[1];
+    if (N.periodic & 1)
+        if (p.x < 0.0) p.x = N.box[0];
+    if (N.periodic & 4)
+        if (p.z > N.box[2]) p.z = 0.0;
+    if (N.periodic & 2)
+        if (p.y > N.box[1]) p.y = 0.0;
+    if (N.periodic & 1)
+        if (p.x > N.box[0]) p.x = 0.0;
+}
+
+template <bool DAMP, bool DRIFT, bool STORE_V>
+__global__ void __launch_bounds__(512) k_step(const StepArgs A) {
+    const FnTile t = A.tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    const FnNet& N = A.nets[t.net];
+
+    double4 p = A.pos_in[i];
+    /* base force: damping * v + gravity, then walls (kernel.cl:231-261) */
+    double Fx, Fy, Fz;
+    if (DAMP) {
+        const float4 v = A.vel[i];
+        Fx = N.damping * (double)v.x;
+        Fy = N.damping * (double)v.y;
+        Fz = N.damping * (double)v.z;
+    } else {
+        Fx = 0.0;
+        Fy = 0.0;
+        Fz = 0.0;
+    }
+    Fx += N.g[0];
+    Fy += N.g[1];
+    Fz += N.g[2];
+    if (N.walls) {
+        if ((N.walls & 4) && p.z < 0.0) Fz += p.z * N.wall_k * -1.0;
+        if ((N.walls & 2) && p.y < 0.0) Fy += p.y * N.wall_k * -1.0;
+        if ((N.walls & 1) && p.x < 0.0) Fx += p.x * N.wall_k * -1.0;
+        if ((N.walls & 4) && p.z > N.box[2]) Fz += (p.z - N.box[2]) * N.wall_k * -1.0;
+        if ((N.walls & 2) && p.y > N.box[1]) Fy += (p.y - N.box[1]) * N.wall_k * -1.0;
+        if ((N.walls & 1) && p.x > N.box[0]) Fx += (p.x - N.box[0]) * N.wall_k * -1.0;
+    }
+
+    /* springs */
+    const int se = A.sp_off[i + 1];
+    for (int e = A.sp_off[i]; e < se; ++e) {
+        const int ent = A.sp_ent[e];
+        const int s = ent >> 1;
+        double fx, fy, fz;
+        int broke;
+        if (spring_eval(A, s, fx, fy, fz, broke)) {
+            if ((ent & 1) == 0) {
+                Fx += fx;
+                Fy += fy;
+                Fz += fz;
+            } else {
+                Fx += fx * -1.0;
+                Fy += fy * -1.0;
+                Fz += fz * -1.0;
+            }
+        }
+        if (broke && (ent & 1) == 0) A.sp_status[s] = 0;
+    }
+
+    /* angles */
+    const int ae = A.an_off[i + 1];
+    for (int e = A.an_off[i]; e < ae; ++e) {
+        const int ent = A.an_ent[e];
+        const int a = ent >> 2;
+        const int role = ent & 3;
+        if (A.an_status[a] != 1) continue;
+        const int4 b = A.an_b[a];
+        if (b.w == 1) {
+            const int2 ss = A.an_s[a];
+            if (!spring_alive_after(A, ss.x) || !spring_alive_after(A, ss.y)) {
+                if (role == 1) A.an_status[a] = 0;
+                continue;
+            }
+        }
+        double pax, pay, paz, pcx, pcy, pcz;
+        angle_eval(A, b, A.an_par[a], pax, pay, paz, pcx, pcy, pcz);
+        if (role == 0) {
+            Fx += pax;
+            Fy += pay;
+            Fz += paz;
+        } else if (role == 2) {
+            Fx += pcx;
+            Fy += pcy;
+            Fz += pcz;
+        } else {
+            Fx += -pax - pcx;
+            Fy += -pay - pcy;
+            Fz += -paz - pcz;
+        }
+    }
+
+    /* contacts */
+    int n = A.list_count[i];
+    if (n > A.list_cap) n = A.list_cap;
+    const int* __restrict__ lst = A.list + i;
+    for (int k = 0; k < n; ++k) {
+        const int j = lst[(size_t)k * A.list_stride];
+        double Rx, Ry, Rz;
+        if (contact_eval(N, A.pairs, p, A.pos_in[j], Rx, Ry, Rz)) {
+            Fx += Rx;
+            Fy += Ry;
+            Fz += Rz;
+        }
+    }
+
+    const float fx = (float)Fx, fy = (float)Fy, fz = (float)Fz;
+    if (!(isfinite(fx) && isfinite(fy) && isfinite(fz)))
+        atomicAdd(A.counters + FN_CNT_NONFINITE, 1ull);
+
+    /* AdvanceVelocity, kernel.cl:451-462 */
+    double4 im = A.img_in[i];
+    const double minv = im.w;
+    const double half_dt = N.half_dt * minv;
+    const float4 fo = A.force[i];
+    const float4 vo = A.vold[i];
+    double tx = (double)fx, ty = (double)fy, tz = (double)fz;
+    tx += (double)fo.x;
+    ty += (double)fo.y;
+    tz += (double)fo.z;
+    const float vox = (float)(tx * half_dt + (double)vo.x);
+    const float voy = (float)(ty * half_dt + (double)vo.y);
+    const float voz = (float)(tz * half_dt + (double)vo.z);
+    A.force[i] = make_float4(fx, fy, fz, 0.0f);
+    A.vold[i] = make_float4(vox, voy, voz, 0.0f);
+
+    if (DRIFT) {
+        float4 v;
+        drift(N, minv, fx, fy, fz, vox, voy, voz, p, im, v);
+        A.pos_out[i] = p;
+        A.img_out[i] = im;
+        if (DAMP || STORE_V) A.vel[i] = v;
+    }
+}
+
+template <bool STORE_V>
+__global__ void __launch_bounds__(512) k_drift(const StepArgs A) {
+    const FnTile t = A.tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    const FnNet& N = A.nets[t.net];
+    double4 p = A.pos_in[i];
+    double4 im = A.img_in[i];
+    const float4 f = A.force[i];
+    const float4 vo = A.vold[i];
+    float4 v;
+    drift(N, im.w, f.x, f.y, f.z, vo.x, vo.y, vo.z, p, im, v);
+    A.pos_out[i] = p;
+    A.img_out[i] = im;
+    if (STORE_V) A.vel[i] = v;
+}
+
+/* Forces alone (no base, no kick, no drift), selected terms; for the
+   one-step force parity checks.  Writes force and the bond statuses. */
+__global__ void k_forces_only(const StepArgs A, int terms) {
+    const FnTile t = A.tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    const FnNet& N = A.nets[t.net];
+    const double4 p = A.pos_in[i];
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    if (terms & 1) {
+        for (int e = A.sp_off[i]; e < A.sp_off[i + 1]; ++e) {
+            const int ent = A.sp_ent[e];
+            double fx, fy, fz;
+            int broke;
+            if (spring_eval(A, ent >> 1, fx, fy, fz, broke)) {
+                const double sg = (ent & 1) ? -1.0 : 1.0;
+                Fx += fx * sg;
+                Fy += fy * sg;
+                Fz += fz * sg;
+            }
+        }
+    }
+    if (terms & 2) {
+        for (int e = A.an_off[i]; e < A.an_off[i + 1]; ++e) {
+            const int ent = A.an_ent[e];
+            const int a = ent >> 2, role = ent & 3;
+            if (A.an_status[a] != 1) continue;
+            const int4 b = A.an_b[a];
+            if (b.w == 1) {
+                const int2 ss = A.an_s[a];
+                if (!spring_alive_after(A, ss.x) || !spring_alive_after(A, ss.y)) continue;
+            }
+            double pax, pay, paz, pcx, pcy, pcz;
+            angle_eval(A, b, A.an_par[a], pax, pay, paz, pcx, pcy, pcz);
+            if (role == 0) {
+                Fx += pax; Fy += pay; Fz += paz;
+            } else if (role == 2) {
+                Fx += pcx; Fy += pcy; Fz += pcz;
+            } else {
+                Fx += -pax - pcx; Fy += -pay - pcy; Fz += -paz - pcz;
+            }
+        }
+    }
+    if (terms & 4) {
+        int n = A.list_count[i];
+        if (n > A.list_cap) n = A.list_cap;
+        for (int k = 0; k < n; ++k) {
+            const int j = A.list[(size_t)k * A.list_stride + i];
+            double Rx, Ry, Rz;
+            if (contact_eval(N, A.pairs, p, A.pos_in[j], Rx, Ry, Rz)) {
+                Fx += Rx; Fy += Ry; Fz += Rz;
+            }
+        }
+    }
+    A.force[i] = make_float4((float)Fx, (float)Fy, (float)Fz, 0.0f);
+}
+
+/* ResetBeadEnergy, kernel.cl:468-483. */
+__global__ void k_reset_energy(float4* force, float4* vel, float4* vold, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    force[i] = z;
+    vel[i] = z;
+    vold[i] = z;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Contact-list rebuild                                                      */
+
+/* FillGrid's cell computation (kernel.cl:492-501) + per-cell counting. */
+__global__ void k_cells(const RebuildArgs R) {
+    const FnTile t = R.tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    const FnNet& N = R.nets[t.net];
+    const double4 p = R.pos[i];
+    const double qx = floor(p.x / N.step[0]);
+    const double qy = floor(p.y / N.step[1]);
+    const double qz = floor(p.z / N.step[2]);
+    int cell = -1;
+    if (qx >= 0.0 && qx < (double)N.nx && qy >= 0.0 && qy < (double)N.ny && qz >= 0.0 &&
+        qz < (double)N.nz) {
+        cell = N.cell_base + (int)qx + (int)qy * N.nx + (int)qz * N.nxy;
+        atomicAdd(R.cell_count + cell, 1);
+    }
+    R.cell_of[i] = cell;
+}
+
+__global__ void k_scatter(const RebuildArgs R, int nb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    const int c = R.cell_of[i];
+    if (c < 0) return;
+    const int slot = atomicAdd(R.cell_fill + c, 1);
+    R.cell_beads[R.cell_start[c] + slot] = i;
+}
+
+/* Orders each cell's beads by index (the order a one-thread FillGrid sweep
+   would store them in) and drops the ones beyond the cell capacity, like the
+   `old < GRID_TAIL_SIZE` test of kernel.cl:503. */
+__global__ void k_cell_sort(const RebuildArgs R, int ncells) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    const int n = R.cell_count[c];
+    if (n <= 1) return;
+    int* b = R.cell_beads + R.cell_start[c];
+    /* selection of the first min(n, cap) positions: ascending order there,
+       O(cap * n) even for an overfull cell */
+    const int keep = n < R.cell_cap ? n : R.cell_cap;
+    for (int k = 0; k < keep; ++k) {
+        int best = k;
+        for (int m = k + 1; m < n; ++m)
+            if (b[m] < b[best]) best = m;
+        const int v = b[best];
+        b[best] = b[k];
+        b[k] = v;
+    }
+    if (n > R.cell_cap) {
+        for (int k = R.cell_cap; k < n; ++k) R.cell_of[b[k]] = -1;
+        atomicAdd(R.counters + FN_CNT_CELL_OVERFLOW, (unsigned long long)(n - R.cell_cap));
+    }
+}
+
+/* Candidate test of BuildContactList (kernel.cl:574-659) for (i, j). */
+__device__ __forceinline__ bool list_candidate(const FnNet& N, const FnPair* __restrict__ pairs,
+                                               double4 pi, int4 bi, double4 pj, int4 bj) {
+    bool collidable = false;
+    if (bi.x != bj.x)
+        collidable = true;
+    else if (abs(bi.y - bj.y) > 1)
+        collidable = true;
+    if (!collidable) return false;
+    double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+    double length = rx * rx + ry * ry + rz * rz;
+    if (N.list_mi) length = min_image(N, rx, ry, rz, length, N.list_mi);
+    const int pid = N.pair_base + getadress(bi.z, bj.z, N.types_num);
+    const int kind = pairs[pid].kind;
+    if (kind == 1 || kind == 3) {
+        if (length < N.cutoff_sq) return true;
+    }
+    if (kind == 2) {
+        const double si = (double)__int_as_float(bi.w), sj = (double)__int_as_float(bj.w);
+        const double ri = (double)w_radius(pi.w), rj = (double)w_radius(pj.w);
+        const double min_skin = (si > sj) ? sj : si;
+        const double max_radius = (ri > rj) ? ri : rj;
+        const double lim = max_radius + min_skin;
+        if (length < lim * lim) return true;
+    }
+    return false;
+}
+
+/* Full per-bead lists over the 27-cell neighbourhood (dz, dy, dx ascending,
+   beads ascending within a cell): the symmetric closure of the reference's
+   half-shell pair set, in a fixed order. */
+__global__ void k_lists(const RebuildArgs R) {
+    const FnTile t = R.tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    const int c = R.cell_of[i];
+    int n = 0;
+    if (c >= 0) {
+        const FnNet& N = R.nets[t.net];
+        const double4 pi = R.pos[i];
+        const int4 bi = R.binfo[i];
+        const int lc = c - N.cell_base;
+        const int cz = lc / N.nxy;
+        const int cy = (lc - cz * N.nxy) / N.nx;
+        const int cx = lc - cz * N.nxy - cy * N.nx;
+        int* __restrict__ out = R.list + i;
+        for (int dz = -1; dz <= 1; ++dz) {
+            int z = cz + dz;
+            if (z < 0 || z >= N.nz) {
+                if (!(N.periodic & 4)) continue;
+                z = z < 0 ? N.nz - 1 : 0;
+            }
+            for (int dy = -1; dy <= 1; ++dy) {
+                int y = cy + dy;
+                if (y < 0 || y >= N.ny) {
+                    if (!(N.periodic & 2)) continue;
+                    y = y < 0 ? N.ny - 1 : 0;
+                }
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int x = cx + dx;
+                    if (x < 0 || x >= N.nx) {
+                        if (!(N.periodic & 1)) continue;
+                        x = x < 0 ? N.nx - 1 : 0;
+                    }
+                    const int nc = N.cell_base + x + y * N.nx + z * N.nxy;
+                    int m = R.cell_count[nc];
+                    if (m > R.cell_cap) m = R.cell_cap;
+                    const int* ids = R.cell_beads + R.cell_start[nc];
+                    for (int k = 0; k < m; ++k) {
+                        const int j = ids[k];
+                        if (j == i) continue;
+                        if (list_candidate(N, R.pairs, pi, bi, R.pos[j], R.binfo[j])) {
+                            if (n < R.list_cap) out[(size_t)n * R.list_stride] = j;
+                            ++n;
+                        }
+                    }
+                }
+            }
+        }
+        if (n > R.list_cap)
+            atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
+    }
+    R.list_count[i] = n;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Exclusive scan of int counts (1024 threads x 2 items per block).          */
+
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 2;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = warp_sums[lane];
+        int s = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        warp_sums[lane] = s - w;
+        if (lane == 31) warp_sums[32] = s;
+    }
+    __syncthreads();
+    total = warp_sums[32];
+    const int r = x - v + warp_sums[warp];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_partials(const int* in, long long n,
+                                                                 int* block_sums) {
+    __shared__ int ws[33];
+    const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k)
+        if (base + k < n) s += in[base + k];
+    int total;
+    block_exclusive_scan(s, ws, total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+/* One block scans the block sums in chunks, carrying the running total. */
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int* block_sums, int nblocks,
+                                                             int* grand_total) {
+    __shared__ int ws[33];
+    int carry = 0;
+    for (int base = 0; base < nblocks; base += SCAN_THREADS) {
+        const int idx = base + (int)threadIdx.x;
+        const int v = idx < nblocks ? block_sums[idx] : 0;
+        int total;
+        const int ex = block_exclusive_scan(v, ws, total);
+        if (idx < nblocks) block_sums[idx] = ex + carry;
+        carry += total;
+    }
+    if (threadIdx.x == 0) *grand_total = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int* in, long long n,
+                                                              const int* block_sums, int* out) {
+    __shared__ int ws[33];
+    const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        s += v[k];
+    }
+    int total;
+    int ex = block_exclusive_scan(s, ws, total) + block_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Observables: deterministic two-pass FP64 reduction per network.           */
+
+__global__ void k_observe_partial(const ObserveArgs O) {
+    __shared__ double sx[256], sy[256], sz[256];
+    __shared__ long long sb[256], sa[256];
+    const int tid = threadIdx.x;
+    double x = 0.0, y = 0.0, z = 0.0;
+    long long nb = 0, na = 0;
+    for (int i = O.bead_begin + blockIdx.x * blockDim.x + tid; i < O.bead_end;
+         i += gridDim.x * blockDim.x) {
+        if (w_type(O.pos[i].w) == O.reaction_type) {
+            const float4 f = O.force[i];
+            x += (double)f.x;
+            y += (double)f.y;
+            z += (double)f.z;
+        }
+    }
+    for (int s = O.spring_begin + blockIdx.x * blockDim.x + tid; s < O.spring_end;
+         s += gridDim.x * blockDim.x)
+        nb += O.sp_status[s] == 0;
+    for (int a = O.angle_begin + blockIdx.x * blockDim.x + tid; a < O.angle_end;
+         a += gridDim.x * blockDim.x)
+        na += O.an_status[a] == 0;
+    sx[tid] = x;
+    sy[tid] = y;
+    sz[tid] = z;
+    sb[tid] = nb;
+    sa[tid] = na;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (tid < o) {
+            sx[tid] += sx[tid + o];
+            sy[tid] += sy[tid + o];
+            sz[tid] += sz[tid + o];
+            sb[tid] += sb[tid + o];
+            sa[tid] += sa[tid + o];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        double* o = O.partial + 5 * (size_t)blockIdx.x;
+        o[0] = sx[0];
+        o[1] = sy[0];
+        o[2] = sz[0];
+        o[3] = (double)sb[0];
+        o[4] = (double)sa[0];
+    }
+}
+
+__global__ void k_observe_final(const double* partial, int nblocks, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < nblocks; ++b)
+        for (int k = 0; k < 5; ++k) a[k] += partial[5 * (size_t)b + k];
+    for (int k = 0; k < 5; ++k) out[k] = a[k];
+}
+
+/* ------------------------------------------------------------------------ */
+/* launch wrappers                                                           */
+
+cudaError_t launch_step(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
+                        bool store_v, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    if (damp) {
+        if (do_drift)
+            k_step<true, true, true><<<ntiles, block, 0, s>>>(A);
+        else
+            k_step<true, false, false><<<ntiles, block, 0, s>>>(A);
+    } else {
+        if (do_drift) {
+            if (store_v)
+                k_step<false, true, true><<<ntiles, block, 0, s>>>(A);
+            else
+                k_step<false, true, false><<<ntiles, block, 0, s>>>(A);
+        } else {
+            k_step<false, false, false><<<ntiles, block, 0, s>>>(A);
+        }
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_drift(const StepArgs& A, int ntiles, int block, bool store_v, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    if (store_v)
+        k_drift<true><<<ntiles, block, 0, s>>>(A);
+    else
+        k_drift<false><<<ntiles, block, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forces_only(const StepArgs& A, int ntiles, int block, int terms,
+                               cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    k_forces_only<<<ntiles, block, 0, s>>>(A, terms);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_energy(float4* force, float4* vel, float4* vold, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_reset_energy<<<(n + 255) / 256, 256, 0, s>>>(force, vel, vold, n);
+    return cudaGetLastError();
+}
+
+long long scan_block_count(long long n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
+
+cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, long long ncells,
+                           int* scan_block_sums, cudaStream_t s) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(R.cell_count, 0, sizeof(int) * (size_t)ncells, s))) return e;
+    if ((e = cudaMemsetAsync(R.cell_fill, 0, sizeof(int) * (size_t)ncells, s))) return e;
+    if (ntiles > 0) k_cells<<<ntiles, block, 0, s>>>(R);
+    const long long nblk = scan_block_count(ncells);
+    k_scan_partials<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(scan_block_sums, (int)nblk, R.cell_start + ncells);
+    k_scan_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums,
+                                                          R.cell_start);
+    if (nb > 0) k_scatter<<<(nb + 255) / 256, 256, 0, s>>>(R, nb);
+    k_cell_sort<<<(unsigned)((ncells + 255) / 256), 256, 0, s>>>(R, (int)ncells);
+    if (ntiles > 0) k_lists<<<ntiles, block, 0, s>>>(R);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_observe(const ObserveArgs& O, int nblocks, double* out, cudaStream_t s) {
+    k_observe_partial<<<nblocks, 256, 0, s>>>(O);
+    k_observe_final<<<1, 32, 0, s>>>(O.partial, nblocks, out);
+    return cudaGetLastError();
+}
+
+}  // namespace fn

@@ -63,8 +63,29 @@ def place_fibres(rng, n_fibres, beads, box, periodic, z_range=None, tilt_deg=5.0
             out[done:done + len(pts)] = pts
             done += len(pts)
         return out
-    return _place_separated(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg, orient, off,
-                            float(min_sep), max_tries)
+    return _place_separated_native(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg,
+                                   orient, spacing, float(min_sep), max_tries)
+
+
+def _place_separated_native(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg, orient,
+                            spacing, rmin, max_tries):
+    """The separated placement in the native library (fn_place_fibres, same
+    algorithm as _place_separated, about 100x faster)."""
+    import ctypes as C
+
+    from . import native
+    lib = native.load()
+    out = np.zeros((n_fibres, beads, 3), np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    mask = sum(1 << a for a in range(3) if periodic[a])
+    seed = int(rng.integers(0, 2**63 - 1))
+    rc = lib.fn_place_fibres(seed, n_fibres, beads, b.ctypes.data_as(C.POINTER(C.c_double)), mask,
+                             float(zlo), float(zhi), float(tilt_deg), 1 if orient == "sphere" else 0,
+                             float(spacing), rmin, int(max_tries),
+                             out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"fibre placement failed (code {rc}) at separation {rmin}")
+    return out
 
 
 def _place_separated(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg, orient, off, rmin,

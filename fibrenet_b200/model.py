@@ -121,8 +121,10 @@ class Model:
 
     def normalised(self) -> "Model":
         """Same model with every array in the dtype and layout the native
-        layers expect (contiguous int32 / float64)."""
-        m = self.copy()
+        layers expect (contiguous int32 / float64); arrays already in that
+        form are shared, not copied."""
+        m = dataclasses.replace(self, settings=dataclasses.replace(self.settings),
+                                type_names=list(self.type_names), meta=dict(self.meta))
         ints = ["pair_kind", "type", "tag", "loc_id", "s_type", "s_tag", "s_p1", "s_p2",
                 "a_type", "a_tag", "a_b1", "a_b2", "a_b3", "a_s1", "a_s2"]
         for name in ints:
@@ -174,3 +176,18 @@ def model_from_arrays(d, prefix: str = "m_") -> Model:
     s["box"] = tuple(s["box"])
     kw = {k: np.array(d[prefix + k]) for k in _ARRAYS}
     return Model(settings=Settings(**s), type_names=json.loads(str(d[prefix + "type_names"])), **kw)
+
+
+def permute_model(m: Model, perm) -> Model:
+    """Model with beads renumbered: new bead q is old bead perm[q]; bond
+    endpoints are remapped, bond order is kept."""
+    m = m.normalised()
+    perm = np.asarray(perm, np.int64)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    out = m.copy()
+    for name in ["type", "tag", "loc_id", "radius", "mass", "pos", "vel", "vel_old", "force", "img"]:
+        setattr(out, name, np.ascontiguousarray(getattr(m, name)[perm]))
+    for name in ["s_p1", "s_p2", "a_b1", "a_b2", "a_b3"]:
+        setattr(out, name, inv[getattr(m, name)].astype(np.int32))
+    return out

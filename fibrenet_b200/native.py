@@ -1,0 +1,308 @@
+"""ctypes binding of libfibrenet.so (the C ABI in include/fibrenet.h).
+
+There is no CPU fallback: if the library or a CUDA device is missing, the
+constructor raises.  Arrays cross the boundary as plain host buffers; the
+context owns all device memory.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .model import Model
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfibrenet.so")
+
+FN_OK = 0
+ERRORS = {1: "bad argument", 2: "CUDA error", 3: "out of device memory", 4: "capacity exceeded",
+          5: "call out of order", 6: "non-finite state", 7: "unsupported"}
+FIELDS = {"pos": 0, "img": 1, "vel": 2, "force": 3, "vel_old": 4}
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+class FnSettings(C.Structure):
+    _fields_ = [("dt", C.c_double), ("lam", C.c_double), ("damping", C.c_double),
+                ("gravity", C.c_double * 3), ("cutoff", C.c_double),
+                ("box_unit_cell", C.c_double), ("box", C.c_double * 3), ("wall_k", C.c_double),
+                ("bc_type", C.c_int), ("grid_update_freq", C.c_int), ("skin_ratio", C.c_double),
+                ("n_types", C.c_int), ("periodic_mask", C.c_int)]
+
+
+class FnNetworkDesc(C.Structure):
+    _fields_ = [("settings", FnSettings), ("pair_kind", _I), ("pair_raw", _D),
+                ("n_beads", C.c_int), ("type", _I), ("tag", _I), ("loc_id", _I),
+                ("radius", _D), ("mass", _D), ("pos", _D), ("vel", _D), ("vel_old", _D),
+                ("force", _D), ("img", _D),
+                ("n_springs", C.c_int), ("s_type", _I), ("s_p1", _I), ("s_p2", _I),
+                ("s_rest", _D), ("s_k", _D), ("s_c1", _D), ("s_c2", _D),
+                ("n_angles", C.c_int), ("a_type", _I), ("a_b1", _I), ("a_b2", _I), ("a_b3", _I),
+                ("a_s1", _I), ("a_s2", _I), ("a_theta0", _D), ("a_k", _D)]
+
+
+class FnConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("cell_capacity", C.c_int), ("list_capacity", C.c_int),
+                ("reorder", C.c_int), ("use_graphs", C.c_int), ("block_size", C.c_int)]
+
+
+class FnStats(C.Structure):
+    _fields_ = [("cell_overflow", C.c_longlong), ("list_overflow", C.c_longlong),
+                ("rebuilds", C.c_longlong), ("steps", C.c_longlong), ("block_size", C.c_int),
+                ("n_networks", C.c_int), ("n_beads", C.c_longlong),
+                ("device_bytes", C.c_longlong)]
+
+
+class FnObservables(C.Structure):
+    _fields_ = [("reaction", C.c_double * 3), ("broken", C.c_longlong),
+                ("angles_dead", C.c_longlong)]
+
+
+# every exported entry point: name -> (restype, argtypes)
+SIGNATURES = {
+    "fn_create": (C.c_int, [C.POINTER(FnConfig), C.POINTER(C.c_void_p)]),
+    "fn_destroy": (None, [C.c_void_p]),
+    "fn_last_error": (C.c_char_p, [C.c_void_p]),
+    "fn_upload": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FnNetworkDesc)]),
+    "fn_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "fn_rebuild_contacts": (C.c_int, [C.c_void_p]),
+    "fn_reset_energy": (C.c_int, [C.c_void_p]),
+    "fn_sync": (C.c_int, [C.c_void_p]),
+    "fn_download": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "fn_set_beads": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "fn_set_mass": (C.c_int, [C.c_void_p, _D]),
+    "fn_set_skin": (C.c_int, [C.c_void_p, _D]),
+    "fn_set_springs": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
+    "fn_set_angles": (C.c_int, [C.c_void_p, _D, _D]),
+    "fn_download_status": (C.c_int, [C.c_void_p, _I, _I]),
+    "fn_set_status": (C.c_int, [C.c_void_p, _I, _I]),
+    "fn_observe": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(FnObservables)]),
+    "fn_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FnStats)]),
+    "fn_get_cells": (C.c_int, [C.c_void_p, _I, _I, C.c_longlong]),
+    "fn_get_lists": (C.c_int, [C.c_void_p, _I, _I, C.c_int]),
+    "fn_n_cells": (C.c_longlong, [C.c_void_p]),
+    "fn_get_permutation": (C.c_int, [C.c_void_p, _I]),
+    "fn_forces_only": (C.c_int, [C.c_void_p, C.c_int]),
+    "fn_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "fn_enable_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "fn_kernel_time": (C.c_int, [C.c_void_p, _D, C.POINTER(C.c_longlong), _D,
+                                 C.POINTER(C.c_longlong)]),
+    "fn_place_fibres": (C.c_int, [C.c_ulonglong, C.c_int, C.c_int, _D, C.c_int, C.c_double,
+                                  C.c_double, C.c_double, C.c_int, C.c_double, C.c_double,
+                                  C.c_int, _D]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the native library (building it first if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        from . import build as _build
+        _build.build()
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Keep:
+    pass
+
+
+def network_desc(m: Model, keep: _Keep) -> FnNetworkDesc:
+    m = m.normalised()
+    keep.__dict__.setdefault("models", []).append(m)
+    s = m.settings
+    d = FnNetworkDesc()
+    st = d.settings
+    st.dt, st.lam, st.damping = s.dt, s.lam, s.damping
+    st.gravity = (C.c_double * 3)(*s.gravity)
+    st.cutoff, st.box_unit_cell = s.cutoff, s.box_unit_cell
+    st.box = (C.c_double * 3)(*s.box)
+    st.wall_k, st.bc_type, st.grid_update_freq = s.wall_k, s.bc_type, s.grid_update_freq
+    st.skin_ratio, st.n_types, st.periodic_mask = s.skin_ratio, m.n_types, s.periodic_mask
+
+    def dp(a):
+        return a.ctypes.data_as(_D)
+
+    def ip(a):
+        return a.ctypes.data_as(_I)
+
+    d.pair_kind, d.pair_raw = ip(m.pair_kind), dp(m.pair_raw)
+    d.n_beads = m.n_beads
+    d.type, d.tag, d.loc_id = ip(m.type), ip(m.tag), ip(m.loc_id)
+    d.radius, d.mass = dp(m.radius), dp(m.mass)
+    d.pos, d.vel, d.vel_old, d.force, d.img = dp(m.pos), dp(m.vel), dp(m.vel_old), dp(m.force), dp(m.img)
+    d.n_springs = m.n_springs
+    d.s_type, d.s_p1, d.s_p2 = ip(m.s_type), ip(m.s_p1), ip(m.s_p2)
+    d.s_rest, d.s_k, d.s_c1, d.s_c2 = dp(m.s_rest), dp(m.s_k), dp(m.s_c1), dp(m.s_c2)
+    d.n_angles = m.n_angles
+    d.a_type, d.a_b1, d.a_b2, d.a_b3 = ip(m.a_type), ip(m.a_b1), ip(m.a_b2), ip(m.a_b3)
+    d.a_s1, d.a_s2, d.a_theta0, d.a_k = ip(m.a_s1), ip(m.a_s2), dp(m.a_theta0), dp(m.a_k)
+    return d
+
+
+class Simulation:
+    """One device context holding one network or a batched ensemble."""
+
+    def __init__(self, models, device: int = 0, cell_capacity: int = 64, list_capacity: int = 64,
+                 reorder: bool = True, use_graphs: bool = False, block_size: int = 0):
+        self.lib = load()
+        self.models = [models] if isinstance(models, Model) else list(models)
+        cfg = FnConfig(device, cell_capacity, list_capacity, int(reorder), int(use_graphs),
+                       block_size)
+        h = C.c_void_p()
+        rc = self.lib.fn_create(C.byref(cfg), C.byref(h))
+        if rc != FN_OK:
+            raise NativeError(rc, "fn_create failed (no CUDA device or bad config)")
+        self.h = h
+        self.list_capacity = list_capacity
+        keep = _Keep()
+        descs = (FnNetworkDesc * len(self.models))(*[network_desc(m, keep) for m in self.models])
+        self._check(self.lib.fn_upload(self.h, len(self.models), descs))
+        self.nb = sum(m.n_beads for m in self.models)
+        self.ns = sum(m.n_springs for m in self.models)
+        self.na = sum(m.n_angles for m in self.models)
+
+    def _check(self, rc):
+        if rc != FN_OK:
+            msg = self.lib.fn_last_error(self.h).decode() if getattr(self, "h", None) else ""
+            raise NativeError(rc, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- stepping
+    def step(self, n: int):
+        self._check(self.lib.fn_step(self.h, int(n)))
+
+    def rebuild(self):
+        self._check(self.lib.fn_rebuild_contacts(self.h))
+
+    def reset_energy(self):
+        self._check(self.lib.fn_reset_energy(self.h))
+
+    def sync(self):
+        self._check(self.lib.fn_sync(self.h))
+
+    def forces_only(self, springs=True, angles=True, contacts=True):
+        terms = (1 if springs else 0) | (2 if angles else 0) | (4 if contacts else 0)
+        self._check(self.lib.fn_forces_only(self.h, terms))
+
+    # --- state
+    def get(self, field: str) -> np.ndarray:
+        out = np.zeros((self.nb, 3), np.float64)
+        self._check(self.lib.fn_download(self.h, FIELDS[field], out.ctypes.data_as(_D)))
+        return out
+
+    def set(self, field: str, values) -> None:
+        a = np.ascontiguousarray(values, np.float64).reshape(self.nb, 3)
+        self._check(self.lib.fn_set_beads(self.h, FIELDS[field], a.ctypes.data_as(_D)))
+
+    def set_mass(self, mass) -> None:
+        a = np.ascontiguousarray(mass, np.float64).reshape(self.nb)
+        self._check(self.lib.fn_set_mass(self.h, a.ctypes.data_as(_D)))
+
+    def set_skin(self, skin) -> None:
+        a = np.ascontiguousarray(skin, np.float64).reshape(self.nb)
+        self._check(self.lib.fn_set_skin(self.h, a.ctypes.data_as(_D)))
+
+    def set_springs(self, rest=None, k=None, c1=None, c2=None) -> None:
+        arrs = [None if x is None else np.ascontiguousarray(x, np.float64).reshape(self.ns)
+                for x in (rest, k, c1, c2)]
+        ptrs = [None if a is None else a.ctypes.data_as(_D) for a in arrs]
+        self._check(self.lib.fn_set_springs(self.h, *ptrs))
+
+    def set_angles(self, theta0=None, k=None) -> None:
+        arrs = [None if x is None else np.ascontiguousarray(x, np.float64).reshape(self.na)
+                for x in (theta0, k)]
+        ptrs = [None if a is None else a.ctypes.data_as(_D) for a in arrs]
+        self._check(self.lib.fn_set_angles(self.h, *ptrs))
+
+    def status(self):
+        s = np.zeros(max(self.ns, 1), np.int32)
+        a = np.zeros(max(self.na, 1), np.int32)
+        self._check(self.lib.fn_download_status(self.h, s.ctypes.data_as(_I), a.ctypes.data_as(_I)))
+        return s[: self.ns], a[: self.na]
+
+    def set_status(self, springs=None, angles=None):
+        s = None if springs is None else np.ascontiguousarray(springs, np.int32)
+        a = None if angles is None else np.ascontiguousarray(angles, np.int32)
+        self._check(self.lib.fn_set_status(self.h, None if s is None else s.ctypes.data_as(_I),
+                                           None if a is None else a.ctypes.data_as(_I)))
+
+    def observe(self, net: int = 0, reaction_type: int = -1) -> dict:
+        o = FnObservables()
+        self._check(self.lib.fn_observe(self.h, net, reaction_type, C.byref(o)))
+        return {"reaction": np.array(o.reaction[:]), "broken": int(o.broken),
+                "angles_dead": int(o.angles_dead)}
+
+    def stats(self) -> dict:
+        s = FnStats()
+        self._check(self.lib.fn_get_stats(self.h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in FnStats._fields_}
+
+    def cells(self):
+        n = int(self.lib.fn_n_cells(self.h))
+        bc = np.zeros(self.nb, np.int32)
+        cc = np.zeros(n, np.int32)
+        self._check(self.lib.fn_get_cells(self.h, bc.ctypes.data_as(_I), cc.ctypes.data_as(_I), n))
+        return bc, cc
+
+    def lists(self):
+        cap = self.list_capacity
+        cnt = np.zeros(self.nb, np.int32)
+        part = np.full((self.nb, cap), -1, np.int32)
+        self._check(self.lib.fn_get_lists(self.h, cnt.ctypes.data_as(_I), part.ctypes.data_as(_I), cap))
+        return cnt, part
+
+    def permutation(self) -> np.ndarray:
+        p = np.zeros(self.nb, np.int32)
+        self._check(self.lib.fn_get_permutation(self.h, p.ctypes.data_as(_I)))
+        return p
+
+    def enable_timing(self, on: bool = True):
+        self._check(self.lib.fn_enable_timing(self.h, int(on)))
+
+    def kernel_time(self):
+        ms = C.c_double()
+        n = C.c_longlong()
+        rms = C.c_double()
+        rn = C.c_longlong()
+        self._check(self.lib.fn_kernel_time(self.h, C.byref(ms), C.byref(n), C.byref(rms), C.byref(rn)))
+        return {"step_ms": ms.value, "launches": n.value, "rebuild_ms": rms.value,
+                "rebuilds": rn.value}
+
+    def autotune(self, steps_per_trial: int = 20) -> int:
+        self._check(self.lib.fn_autotune(self.h, steps_per_trial))
+        return self.stats()["block_size"]

@@ -1,0 +1,238 @@
+/*
+ * fibrenet.h -- C ABI of the B200 FibreNet step loop.
+ *
+ * Replaces the reference's device layer (OpenclManager + BufferIndex, used
+ * only by SimulationManager) with one opaque context per simulation: the
+ * context owns every device buffer, host pointers are borrowed for the
+ * duration of a call, and every entry point returns an int status
+ * (FN_OK = 0) instead of the reference's bool / negative int.  Calls on one
+ * context are not thread-safe; separate contexts are independent.
+ *
+ * Units, field meanings and file semantics are the reference's
+ * (README.md:32-659).  Bead, spring and angle indices are the model-file
+ * order; the context may renumber beads internally but every call here uses
+ * the caller's numbering.
+ */
+#ifndef FIBRENET_H
+#define FIBRENET_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FN_API __attribute__((visibility("default")))
+
+/* status codes */
+enum {
+    FN_OK = 0,
+    FN_ERR_ARG = 1,        /* bad argument (null, size, index out of range) */
+    FN_ERR_CUDA = 2,       /* CUDA runtime error (text in fn_last_error) */
+    FN_ERR_OOM = 3,        /* device allocation failed */
+    FN_ERR_CAPACITY = 4,   /* a cell or contact list exceeded its capacity */
+    FN_ERR_STATE = 5,      /* call out of order (e.g. step before upload) */
+    FN_ERR_NONFINITE = 6,  /* NaN/inf detected in the state */
+    FN_ERR_UNSUPPORTED = 7 /* request outside what this build implements */
+};
+
+/* bead fields for fn_download / fn_set_beads (3 doubles per bead) */
+enum {
+    FN_POSITION = 0,      /* wrapped position, Bead.position */
+    FN_IMAGE = 1,         /* unwrapped position, Bead.image_position */
+    FN_VELOCITY = 2,      /* predicted velocity, Bead.velocity */
+    FN_FORCE = 3,         /* Bead.force */
+    FN_VELOCITY_OLD = 4   /* Bead.velocity_old */
+};
+
+/* pair kinds (SimulationManager.cpp:891-932) */
+enum { FN_PAIR_LJ = 1, FN_PAIR_HS = 2, FN_PAIR_ST = 3 };
+
+typedef struct fn_ctx fn_ctx;
+
+/* Input-file settings of one network, as written in the input file
+   (SimulationManager.cpp:644-819, 2070-2170). */
+typedef struct fn_settings {
+    double dt;            /* 'step' */
+    double lambda;        /* 'lambda' */
+    double damping;       /* 'damping' as written; negated internally (:664) */
+    double gravity[3];    /* 'gravity' */
+    double cutoff;        /* 'cutoff' */
+    double box_unit_cell; /* 'box_unit_cell' */
+    double box[3];        /* 'box_size' */
+    double wall_k;        /* 'box_wall_rep' */
+    int bc_type;          /* 0 pbc, 1 finite (after the :2168 override) */
+    int grid_update_freq; /* 'grid_update_freq' */
+    double skin_ratio;    /* skin_radius = radius + skin_ratio (:1431) */
+    int n_types;          /* number of 'type' lines */
+    int periodic_mask;    /* extension: bit a = axis a periodic; -1 = bc_type */
+} fn_settings;
+
+/* One network's model, borrowed host arrays (model-file order).  Vectors
+   are 3 doubles per bead.  Replaces the CreateBuffer<Bead/BeadInfo/
+   SpringStructure/AngleBond/Pair> uploads of ReadBeadsData, ReadSpringData,
+   ReadAngleData and LoadTypeAndPairInfo (SimulationManager.cpp:1461-1486,
+   1572, 1650, 963). */
+typedef struct fn_network_desc {
+    fn_settings settings;
+    const int* pair_kind;    /* n_types*(n_types+1)/2 entries, GETADRESS order */
+    const double* pair_raw;  /* 4 per pair: the 'pair' line tokens 4..7 */
+    int n_beads;
+    const int* type;
+    const int* tag;
+    const int* loc_id;
+    const double* radius;
+    const double* mass;
+    const double* pos;
+    const double* vel;
+    const double* vel_old;
+    const double* force;
+    const double* img;
+    int n_springs;
+    const int* s_type;       /* 0 HR, 1 HR_FL */
+    const int* s_p1;
+    const int* s_p2;
+    const double* s_rest;
+    const double* s_k;
+    const double* s_c1;      /* HR_FL Young's modulus */
+    const double* s_c2;      /* HR_FL failure stress */
+    int n_angles;
+    const int* a_type;       /* 0 HR, 1 HR_FL */
+    const int* a_b1;
+    const int* a_b2;
+    const int* a_b3;
+    const int* a_s1;
+    const int* a_s2;
+    const double* a_theta0;
+    const double* a_k;
+} fn_network_desc;
+
+typedef struct fn_config {
+    int device;         /* CUDA device ordinal */
+    int cell_capacity;  /* beads kept per grid cell (reference: 64, kernel.cl:10) */
+    int list_capacity;  /* contacts kept per bead (full list) */
+    int reorder;        /* 1: renumber beads in Morton order of their fibre */
+    int use_graphs;     /* 1: replay steps as CUDA graphs */
+    int block_size;     /* threads per block for the step kernel; 0 = tune */
+} fn_config;
+
+/* Counters read back from the device. */
+typedef struct fn_stats {
+    long long cell_overflow;   /* beads dropped because a cell was full */
+    long long list_overflow;   /* contacts dropped because a list was full */
+    long long rebuilds;        /* contact-list rebuilds done */
+    long long steps;           /* time steps done */
+    int block_size;            /* step-kernel block size in use */
+    int n_networks;
+    long long n_beads;
+    long long device_bytes;    /* device memory held by the context */
+} fn_stats;
+
+/* Per-network observables (FP64 reductions on the device). */
+typedef struct fn_observables {
+    double reaction[3];   /* sum of Bead.force over beads of the chosen type */
+    long long broken;     /* springs with status 0 */
+    long long angles_dead;/* angles with status 0 */
+} fn_observables;
+
+/* OpenclManager::Initialize (OpenclManager.cpp:5-85) without the interactive
+   platform/device prompt: binds cfg->device and creates the stream. */
+FN_API int fn_create(const fn_config* cfg, fn_ctx** out);
+
+/* Frees every device buffer (OpenclManager::Close). */
+FN_API void fn_destroy(fn_ctx* ctx);
+
+/* Text of the last error on this context ("" if none).  Replaces checkErr
+   logging (OpenclManager.cpp:335-408). */
+FN_API const char* fn_last_error(const fn_ctx* ctx);
+
+/* Uploads n_networks independent networks (1 = the reference's single
+   simulation; >1 = a batched ensemble run in the same launches).  Replaces
+   the CreateBuffer/WriteBuffer calls of ReadInputFile and the argument binding
+   of ReadKernelData (SimulationManager.cpp:1153-1307; OpenclManager.h:121-174). */
+FN_API int fn_upload(fn_ctx* ctx, int n_networks, const fn_network_desc* nets);
+
+/* RunSimulationLoop(nsteps) on every network (SimulationManager.cpp:151-181):
+   kick/drift, springs, angles, contact rebuild at step 0 of the call and every
+   grid_update_freq steps, contacts, velocity update.  Asynchronous with
+   respect to the host; ExecuteKernel + RunKernels per step become one
+   stream-ordered (optionally graph-replayed) sequence. */
+FN_API int fn_step(fn_ctx* ctx, int nsteps);
+
+/* ResetGrid + ResetContactList + FillGrid + BuildContactList at the current
+   positions (kernel.cl:487-789). */
+FN_API int fn_rebuild_contacts(fn_ctx* ctx);
+
+/* ResetBeadEnergy (kernel.cl:468-483) on every network, as
+   MinimizeSystemEnergy calls it (SimulationManager.cpp:120, 138). */
+FN_API int fn_reset_energy(fn_ctx* ctx);
+
+/* Waits for the context's stream (OpenclManager::RunKernels). */
+FN_API int fn_sync(fn_ctx* ctx);
+
+/* Blocking read of one bead field, 3 doubles per bead, all networks in upload
+   order (OpenclManager::ReadBuffer as DumpData/DumpRestartData use it,
+   SimulationManager.cpp:1996, 1884). */
+FN_API int fn_download(fn_ctx* ctx, int field, double* host);
+
+/* Overwrites one bead field (the read-modify-write of LoadBeadModifications
+   and ReadRestartFile, SimulationManager.cpp:220-228, 403-411, 1739-1816). */
+FN_API int fn_set_beads(fn_ctx* ctx, int field, const double* host);
+
+/* Per-bead mass, all networks in upload order (modif_bead mass,
+   SimulationManager.cpp:267-316): recomputes the inverse-mass constants. */
+FN_API int fn_set_mass(fn_ctx* ctx, const double* mass);
+
+/* Per-bead skin radius (modif_bead skin_radius, SimulationManager.cpp:356-391). */
+FN_API int fn_set_skin(fn_ctx* ctx, const double* skin_radius);
+
+/* Spring parameters, all networks in upload order (modif_spring
+   rest_length/stiffness/c1/c2, SimulationManager.cpp:449-626).  A null
+   pointer leaves that parameter unchanged. */
+FN_API int fn_set_springs(fn_ctx* ctx, const double* rest, const double* k, const double* c1,
+                          const double* c2);
+
+/* Angle stiffness and rest angle (no reference counterpart; used by fitting). */
+FN_API int fn_set_angles(fn_ctx* ctx, const double* theta0, const double* k);
+
+/* Spring and angle status (1 alive, 0 broken/dead), all networks. */
+FN_API int fn_download_status(fn_ctx* ctx, int* spring_status, int* angle_status);
+FN_API int fn_set_status(fn_ctx* ctx, const int* spring_status, const int* angle_status);
+
+/* Observables of network `net`; reaction sums the force on beads of type
+   `reaction_type` (-1: none). */
+FN_API int fn_observe(fn_ctx* ctx, int net, int reaction_type, fn_observables* out);
+
+FN_API int fn_get_stats(fn_ctx* ctx, fn_stats* out);
+
+/* Grid and contact-list inspection (tests): cell of each bead (-1 outside
+   the grid or beyond the cell capacity), the raw count of each cell, and
+   each bead's contacts (raw count and up to cap partner ids), all in upload
+   numbering; cells are numbered per network like the reference
+   (x + y*nx + z*nx*ny) plus the network's cell offset. */
+FN_API int fn_get_cells(fn_ctx* ctx, int* bead_cell, int* cell_count, long long n_cells);
+FN_API int fn_get_lists(fn_ctx* ctx, int* count, int* partners, int cap);
+FN_API long long fn_n_cells(fn_ctx* ctx);
+
+/* Forces alone at the current positions and contact list (zeroed first, no
+   damping/gravity/wall term, no kick or drift): the per-step force of
+   ResolveSprings + ResolveAngles + ResolveContacts (kernel.cl:268-441,
+   792-1011) for one-step parity checks.  terms: bit 0 springs, 1 angles,
+   2 contacts.  The result is read with fn_download(FN_FORCE). */
+FN_API int fn_forces_only(fn_ctx* ctx, int terms);
+
+/* Internal bead numbering: perm[internal] = upload index. */
+FN_API int fn_get_permutation(fn_ctx* ctx, int* perm);
+
+/* Time the step kernel at each candidate block size and keep the fastest
+   (state is snapshotted and restored). */
+FN_API int fn_autotune(fn_ctx* ctx, int steps_per_trial);
+
+/* Average duration (ms) of the step kernel over the last fn_step call when
+   timing is enabled, with the launch count. */
+FN_API int fn_enable_timing(fn_ctx* ctx, int on);
+FN_API int fn_kernel_time(fn_ctx* ctx, double* step_kernel_ms, long long* launches,
+                          double* rebuild_ms, long long* rebuilds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

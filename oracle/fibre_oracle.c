@@ -31,6 +31,9 @@
 
 #include "oracle_host.h"
 #include "oracle_model.h"
+/* MIRROR mode uses the device path's arc cosine (IEEE ops only), so both
+   sides round identically; REF mode keeps libm acos like kernel.cl:314. */
+#include "fn_detmath.h"
 
 #define FO_EXPORT __attribute__((visibility("default")))
 
@@ -372,7 +375,7 @@ static void angle_force(const fo_ctx* c, int a, double pa[3], double pc[3]) {
     double dotp = (ba[0] * bc[0] + ba[1] * bc[1] + ba[2] * bc[2]) / (l_ba * l_bc);
     if (dotp < -1.0) dotp = -0.999999;
     if (dotp > 1.0) dotp = 0.999999;
-    double angle = acos(dotp);
+    double angle = c->mode == FO_MODE_MIRROR ? fn_acos(dotp) : acos(dotp);
     double magnitude = -2.0 * c->a_k[a] * (angle - c->a_theta0[a]);
     double fa = magnitude / l_ba;
     double fc = magnitude / l_bc;
@@ -831,6 +834,8 @@ FO_EXPORT void fo_get_lists(const fo_ctx* c, int* head, int* partners, int* pair
     if (partners) memcpy(partners, c->list_j, sizeof(int) * (size_t)c->nb * (size_t)c->list_cap);
     if (pairs) memcpy(pairs, c->list_pair, sizeof(int) * (size_t)c->nb * (size_t)c->list_cap);
 }
+
+FO_EXPORT double fo_detmath_acos(double x) { return fn_acos(x); }
 
 FO_EXPORT void fo_overflow(const fo_ctx* c, long* out2) {
     out2[0] = c->overflow_cells;

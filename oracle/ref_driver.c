@@ -61,7 +61,7 @@ typedef struct ref_ctx {
             }                                                                        \
         } else {                                                                     \
             int nt_ = (ctx)->threads;                                                \
-            _Pragma("omp parallel for num_threads(nt_) schedule(dynamic, 256)")      \
+            _Pragma("omp parallel for num_threads(nt_) schedule(static)")      \
             for (int g_ = 0; g_ < n_; ++g_) {                                        \
                 fn_cl_global_id = g_;                                                \
                 call;                                                                \

@@ -1,0 +1,202 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+* bit-exact against the oracle's MIRROR mode (same storage rounding and
+  summation order) on every golden case, including bond statuses;
+* within FP32 storage rounding of the reference's own results (golden
+  vectors from kernel.cl) on the same cases;
+* identical grid cells and contact-pair sets to the reference;
+* one-step forces within 1e-5 (norm-wise) of the FP64 reference;
+* bit-exact broken-spring sets over 1,000 steps of a tensile pull.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import GOLDEN, golden_cases
+from fibrenet_b200 import generate as g
+from fibrenet_b200.model import model_from_arrays, permute_model
+from gpu_util import FIELDS, rel_norm, run_seq
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5  # relative, norm-wise, FP32 result vs FP64 reference
+
+
+def sim(model, **kw):
+    from fibrenet_b200.native import Simulation
+    kw.setdefault("reorder", False)
+    kw.setdefault("list_capacity", 256)
+    return Simulation(model, **kw)
+
+
+def load(name):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    return d, model_from_arrays(d)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_bit_exact_vs_mirror(oracle_built, name):
+    d, m = load(name)
+    s = sim(m)
+    o = po.OracleSim(m, po.MODE_MIRROR, cell_cap=64, list_cap=256)
+    run_seq(s, d["runs"])
+    run_seq(o, d["runs"])
+    for f in FIELDS:
+        np.testing.assert_array_equal(s.get(f), o.get(f), err_msg=f"{name}: {f}")
+    ss, sa = s.status()
+    os_, oa = o.status()
+    np.testing.assert_array_equal(ss, os_)
+    np.testing.assert_array_equal(sa, oa)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_close_to_reference(name):
+    d, m = load(name)
+    s = sim(m)
+    run_seq(s, d["runs"])
+    ref = d["out_img"]
+    scale = max(1.0, float(np.abs(ref).max()))
+    np.testing.assert_allclose(s.get("img"), ref, rtol=0, atol=2e-5 * scale)
+    np.testing.assert_array_equal(s.status()[0], d["out_spring_status"])
+    np.testing.assert_array_equal(s.status()[1], d["out_angle_status"])
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_cells_and_pairs_match_reference(name):
+    """Cell ids and the contact-pair set built from the reference's final
+    positions equal the reference's own (kernel.cl FillGrid +
+    BuildContactList), bit for bit."""
+    d, m = load(name)
+    m.pos = d["out_pos"]
+    s = sim(m)
+    s.rebuild()
+    bc, cc = s.cells()
+    np.testing.assert_array_equal(cc, d["out_grid_head"])
+    grid = sorted((int(c), i) for i, c in enumerate(bc) if c >= 0)
+    assert grid == [tuple(x) for x in d["out_grid"].tolist()]
+    cnt, part = s.lists()
+    got = sorted(po.pair_set(cnt, part))
+    want = sorted({(int(a), int(b)) for a, b, _ in d["out_pairs"].tolist()})
+    assert got == want
+
+
+def test_one_step_forces_vs_fp64_reference(oracle_built):
+    """Config-0 geometry (200 fibres x 50 beads), identical FP32-representable
+    inputs: springs + angles + penalty contacts of one evaluation."""
+    m = g.plain_network(seed=21).fp32_representable()
+    # a perturbed state so every term is active
+    rng = np.random.default_rng(0)
+    m.img = m.img + rng.normal(0.0, 0.02, m.img.shape)
+    m.img = m.img.astype(np.float32).astype(np.float64)
+    box = np.asarray(m.settings.box)
+    m.pos = np.mod(m.img, box)
+    r = po.OracleSim(m, po.MODE_REF)
+    r.rebuild()
+    r.forces_only()
+    fr = r.get("force")
+    s = sim(m, list_capacity=64)
+    s.rebuild()
+    s.forces_only()
+    fg = s.get("force")
+    err = rel_norm(fg, fr)
+    assert err <= FORCE_TOL, err
+    # each term on its own
+    for terms in [(1, 0, 0), (0, 1, 0), (0, 0, 1)]:
+        r.forces_only(*terms)
+        s.forces_only(*terms)
+        e = rel_norm(s.get("force"), r.get("force"))
+        assert e <= FORCE_TOL, (terms, e)
+
+
+def test_reordered_run_matches_mirror_on_permuted_model(oracle_built):
+    m = g.plain_network(seed=4, fibres=40, beads=25, box=(30.0, 30.0, 6.0), z_range=(1.0, 5.0))
+    s = sim(m, reorder=True, list_capacity=64)
+    perm = s.permutation()
+    assert sorted(perm.tolist()) == list(range(m.n_beads))
+    mp = permute_model(m, perm)
+    o = po.OracleSim(mp, po.MODE_MIRROR, cell_cap=64, list_cap=64)
+    s.step(37)
+    o.run(37)
+    for f in FIELDS:
+        np.testing.assert_array_equal(s.get(f)[perm], o.get(f), err_msg=f)
+
+
+def test_call_cadence_matches_mirror(oracle_built):
+    """The rebuild counter restarts with every call (SimulationManager.cpp:152)."""
+    m = g.plain_network(seed=9, fibres=30, beads=20, box=(25.0, 25.0, 6.0), z_range=(1.0, 5.0))
+    s = sim(m, list_capacity=64)
+    o = po.OracleSim(m, po.MODE_MIRROR, cell_cap=64, list_cap=64)
+    for n in [1, 5, 13, 2, 8]:
+        s.step(n)
+        o.run(n)
+    for f in FIELDS:
+        np.testing.assert_array_equal(s.get(f), o.get(f), err_msg=f)
+
+
+def test_broken_set_1000_steps_bit_exact(oracle_built):
+    """Tensile pull with HR_FL springs: the set of broken springs over 1,000
+    steps equals the mirror oracle's exactly, checked every 100 steps."""
+    m = g.tensile_network(seed=3, fibres=60, beads=30, box=(60.0, 40.0, 10.0), z_range=(1.0, 9.0),
+                          fail_mu=np.log(0.8), fail_sigma=0.4, clamp_lo=2.0, clamp_hi=58.0,
+                          pull=0.5, cell=2.5, min_sep=1.0)
+    s = sim(m, list_capacity=64)
+    o = po.OracleSim(m, po.MODE_MIRROR, cell_cap=64, list_cap=64)
+    for _ in range(10):
+        s.step(100)
+        o.run(100)
+        np.testing.assert_array_equal(s.status()[0], o.status()[0])
+    np.testing.assert_array_equal(s.get("img"), o.get("img"))
+    assert (s.status()[0] == 0).sum() > 0  # the pull does break springs
+
+
+def test_batched_equals_separate_runs():
+    ms = [g.plain_network(seed=30 + k, fibres=10 + 7 * k, beads=20, box=(20.0 + 4 * k, 20.0, 6.0),
+                          z_range=(1.0, 5.0)) for k in range(4)]
+    with sim(ms, list_capacity=64) as b:
+        b.step(25)
+        allpos = b.get("img")
+        st = b.status()[0]
+    off = 0
+    soff = 0
+    for m in ms:
+        with sim(m, list_capacity=64) as one:
+            one.step(25)
+            np.testing.assert_array_equal(allpos[off:off + m.n_beads], one.get("img"))
+            np.testing.assert_array_equal(st[soff:soff + m.n_springs], one.status()[0])
+        off += m.n_beads
+        soff += m.n_springs
+
+
+def test_observables_match_host_sums():
+    m = g.tensile_network(seed=5, fibres=40, beads=20, box=(40.0, 30.0, 8.0), z_range=(1.0, 7.0),
+                          clamp_lo=2.0, clamp_hi=38.0, pull=0.2, cell=2.5)
+    s = sim(m, list_capacity=64)
+    s.step(50)
+    o = s.observe(0, reaction_type=2)
+    f = s.get("force")
+    want = f[m.type == 2].sum(axis=0)
+    np.testing.assert_allclose(o["reaction"], want, rtol=1e-12, atol=1e-12)
+    assert o["broken"] == int((s.status()[0] == 0).sum())
+
+
+def test_reset_energy_and_set_state(oracle_built):
+    m = g.plain_network(seed=12, fibres=10, beads=10, box=(12.0, 12.0, 6.0), z_range=(1.0, 5.0))
+    s = sim(m, list_capacity=64)
+    s.step(5)
+    s.reset_energy()
+    for f in ["vel", "force", "vel_old"]:
+        assert not s.get(f).any()
+    v = np.random.default_rng(1).normal(size=(m.n_beads, 3)).astype(np.float32).astype(np.float64)
+    s.set("vel_old", v)
+    np.testing.assert_array_equal(s.get("vel_old"), v)
+
+
+def test_bad_model_is_rejected():
+    from fibrenet_b200.native import NativeError
+    m = g.plain_network(seed=1, fibres=4, beads=5, box=(10.0, 10.0, 6.0), z_range=(1.0, 5.0))
+    m.s_p2 = m.s_p2.copy()
+    m.s_p2[0] = 10_000
+    with pytest.raises(NativeError):
+        sim(m)
