@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--fibres", type=int, default=20000)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     return p.parse_args()
 
@@ -214,6 +215,59 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def run_e2e(args, m, local, dist, world, nb, barrier):
+    """Same metric through the public API with host buffers: model upload from
+    pinned host arrays, RunSimulationLoop in output_freq chunks with the
+    recorded observables read back after each chunk, final state download."""
+    import torch
+
+    from fibrenet_b200.native import Simulation
+
+    e2e_steps = args.steps
+    pinned = {}
+    mm = m.normalised()
+    for name in ["pos", "img", "vel", "vel_old", "force"]:
+        t = torch.from_numpy(getattr(mm, name)).pin_memory()
+        pinned[name] = t
+        setattr(mm, name, t.numpy())
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    w0 = time.perf_counter()
+    sim2 = Simulation(mm, device=local, list_capacity=64, cell_capacity=64, reorder=True)
+    done = 0
+    obs_bytes = 0
+    while done < e2e_steps:
+        k = min(OUTPUT_FREQ, e2e_steps - done)
+        sim2.step(k)
+        o = sim2.observe(0, reaction_type=2)
+        obs_bytes += 5 * 8
+        done += k
+    final = sim2.get("pos")
+    sim2.sync()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - w0
+    e2e_ms = max(e0.elapsed_time(e1), 1e3 * e2e_wall)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = sum(getattr(mm, k).nbytes for k in ["pos", "img", "vel", "vel_old", "force", "radius", "mass",
+                                            "type", "tag", "loc_id", "s_type", "s_p1", "s_p2",
+                                            "s_rest", "s_k", "s_c1", "s_c2", "a_type", "a_b1",
+                                            "a_b2", "a_b3", "a_s1", "a_s2", "a_theta0", "a_k"])
+    d2h = obs_bytes + final.nbytes
+    e2e_value = world * nb * e2e_steps / (e2e_ms / 1e3)
+    sim2.close()
+    return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+            "d2h_bytes_per_step": d2h / e2e_steps,
+            "what": "Simulation(model from pinned host arrays) + step() in chunks of "
+                    f"{OUTPUT_FREQ} with observe() after each + final get('pos')"}
+
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -277,44 +331,9 @@ def run_ours(args):
     # ---- end to end through the public API: model upload from pinned host
     # buffers, RunSimulationLoop in output_freq chunks with the recorded
     # observables read back after each chunk, final state download
-    e2e_steps = args.steps
-    pinned = {}
-    mm = m.normalised()
-    for name in ["pos", "img", "vel", "vel_old", "force"]:
-        t = torch.from_numpy(getattr(mm, name)).pin_memory()
-        pinned[name] = t
-        setattr(mm, name, t.numpy())
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    w0 = time.perf_counter()
-    sim2 = Simulation(mm, device=local, list_capacity=64, cell_capacity=64, reorder=True)
-    done = 0
-    obs_bytes = 0
-    while done < e2e_steps:
-        k = min(OUTPUT_FREQ, e2e_steps - done)
-        sim2.step(k)
-        o = sim2.observe(0, reaction_type=2)
-        obs_bytes += 5 * 8
-        done += k
-    final = sim2.get("pos")
-    sim2.sync()
-    e1.record()
-    torch.cuda.synchronize()
-    e2e_wall = time.perf_counter() - w0
-    e2e_ms = max(e0.elapsed_time(e1), 1e3 * e2e_wall)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    h2d = sum(getattr(mm, k).nbytes for k in ["pos", "img", "vel", "vel_old", "force", "radius", "mass",
-                                            "type", "tag", "loc_id", "s_type", "s_p1", "s_p2",
-                                            "s_rest", "s_k", "s_c1", "s_c2", "a_type", "a_b1",
-                                            "a_b2", "a_b3", "a_s1", "a_s2", "a_theta0", "a_k"])
-    d2h = obs_bytes + final.nbytes
-    e2e_value = world * nb * e2e_steps / (e2e_ms / 1e3)
-    sim2.close()
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, m, local, dist, world, nb, barrier)
 
     peak, peak_kind = peaks()
     alg = algorithmic_bytes(m, half_pairs)
@@ -346,10 +365,7 @@ def run_ours(args):
                          "step_kernel_ms": step_ms, "rebuild_ms": kt["rebuild_ms"],
                          "traffic": (traffic_per_bead * nb) if traffic_per_bead else None},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
-                    "d2h_bytes_per_step": d2h / e2e_steps,
-                    "what": "Simulation(model from pinned host arrays) + step() in chunks of "
-                            f"{OUTPUT_FREQ} with observe() after each + final get('pos')"},
+            "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clk,
             "overflow": {"cell": stats["cell_overflow"], "list": stats["list_overflow"]},

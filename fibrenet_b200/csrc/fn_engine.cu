@@ -38,7 +38,18 @@ struct NetHost {
     long long cell_begin, cell_end;
     int grid_update_freq;
     double damping;
+    bool any_cut, any_hs; /* pair kinds present (listing radius) */
+    double rmax;          /* largest radius, as stored */
 };
+
+/* Largest listing radius squared of one network (kernel.cl:632-650): the
+   cutoff for lj/st pairs, largest radius + largest skin for hs pairs. */
+double list_r2(const NetHost& h, double cutoff_sq, double smax) {
+    double r2 = 0.0;
+    if (h.any_cut) r2 = cutoff_sq;
+    if (h.any_hs) r2 = std::max(r2, (h.rmax + smax) * (h.rmax + smax));
+    return r2;
+}
 
 int getadress_h(int t1, int t2, int size) {
     return (t1 < t2) ? ((size * t1) + t2 - ((t1 * (t1 + 1)) / 2))
@@ -86,6 +97,15 @@ struct fn_ctx {
     DevBuf<float2> an_par;
     DevBuf<signed char> an_status;
     DevBuf<int> sp_off, sp_ent, an_off, an_ent;
+    /* host copies of the incidence (internal numbering) for the tile lists */
+    std::vector<int> sp_off_h, sp_ent_h, an_off_h, an_ent_h;
+    std::vector<int4> an_b_h;
+    std::vector<int2> an_s_h;
+    /* per-tile bonded term lists of the tiled step kernel */
+    DevBuf<int> tile_sp_off, tile_sp, tile_an_off, tile_an, sp_slot, an_slot;
+    DevBuf<int2> tile_an_sslot;
+    int max_tile_sp = 0, max_tile_an = 0;
+    bool tiled = false;
     DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
     DevBuf<int> scan_sums;
     DevBuf<FnTile> tiles;
@@ -171,6 +191,13 @@ void free_all(fn_ctx* c) {
     dfree(c, c->an_s);
     dfree(c, c->an_par);
     dfree(c, c->an_status);
+    dfree(c, c->tile_sp_off);
+    dfree(c, c->tile_sp);
+    dfree(c, c->tile_an_off);
+    dfree(c, c->tile_an);
+    dfree(c, c->sp_slot);
+    dfree(c, c->an_slot);
+    dfree(c, c->tile_an_sslot);
     dfree(c, c->sp_off);
     dfree(c, c->sp_ent);
     dfree(c, c->an_off);
@@ -350,11 +377,90 @@ int build_tiles(fn_ctx* c, int block, std::vector<FnTile>& out) {
     return (int)out.size();
 }
 
+/* Bonded terms of each tile (springs and angles incident to its beads, plus
+   the two springs of every HR_FL angle, whose break test decides the angle),
+   and the per-bead entries rewritten as tile slots. */
+int build_tile_terms(fn_ctx* c, const std::vector<FnTile>& tiles) {
+    const size_t nt = tiles.size();
+    std::vector<int> tsp_off(nt + 1, 0), tan_off(nt + 1, 0), tsp, tan;
+    std::vector<int2> sslot;
+    std::vector<int> sp_slot(c->sp_ent_h.size()), an_slot(c->an_ent_h.size());
+    int max_sp = 0, max_an = 0;
+    std::vector<int> ls, la;
+    for (size_t t = 0; t < nt; ++t) {
+        ls.clear();
+        la.clear();
+        for (int i = tiles[t].begin; i < tiles[t].end; ++i) {
+            for (int e = c->sp_off_h[i]; e < c->sp_off_h[i + 1]; ++e) ls.push_back(c->sp_ent_h[e] >> 1);
+            for (int e = c->an_off_h[i]; e < c->an_off_h[i + 1]; ++e) la.push_back(c->an_ent_h[e] >> 2);
+        }
+        std::sort(la.begin(), la.end());
+        la.erase(std::unique(la.begin(), la.end()), la.end());
+        for (int a : la)
+            if (c->an_b_h[a].w == 1) {
+                ls.push_back(c->an_s_h[a].x);
+                ls.push_back(c->an_s_h[a].y);
+            }
+        std::sort(ls.begin(), ls.end());
+        ls.erase(std::unique(ls.begin(), ls.end()), ls.end());
+        auto slot_of = [](const std::vector<int>& v, int x) {
+            return (int)(std::lower_bound(v.begin(), v.end(), x) - v.begin());
+        };
+        for (int i = tiles[t].begin; i < tiles[t].end; ++i) {
+            for (int e = c->sp_off_h[i]; e < c->sp_off_h[i + 1]; ++e) {
+                const int ent = c->sp_ent_h[e];
+                sp_slot[e] = (slot_of(ls, ent >> 1) << 1) | (ent & 1);
+            }
+            for (int e = c->an_off_h[i]; e < c->an_off_h[i + 1]; ++e) {
+                const int ent = c->an_ent_h[e];
+                an_slot[e] = (slot_of(la, ent >> 2) << 2) | (ent & 3);
+            }
+        }
+        for (int a : la) {
+            if (c->an_b_h[a].w == 1)
+                sslot.push_back(make_int2(slot_of(ls, c->an_s_h[a].x), slot_of(ls, c->an_s_h[a].y)));
+            else
+                sslot.push_back(make_int2(0, 0));
+        }
+        tsp.insert(tsp.end(), ls.begin(), ls.end());
+        tan.insert(tan.end(), la.begin(), la.end());
+        tsp_off[t + 1] = (int)tsp.size();
+        tan_off[t + 1] = (int)tan.size();
+        max_sp = std::max(max_sp, (int)ls.size());
+        max_an = std::max(max_an, (int)la.size());
+    }
+    const size_t smem = fn::step_tiled_smem(max_sp, max_an);
+    c->tiled = smem <= 160 * 1024;
+    if (!c->tiled) return FN_OK;
+    CK(fn::prepare_step_tiled(smem));
+    CK(dalloc(c, c->tile_sp_off, tsp_off.size()));
+    CK(dalloc(c, c->tile_an_off, tan_off.size()));
+    CK(dalloc(c, c->tile_sp, tsp.size()));
+    CK(dalloc(c, c->tile_an, tan.size()));
+    CK(dalloc(c, c->tile_an_sslot, sslot.size()));
+    CK(dalloc(c, c->sp_slot, sp_slot.size()));
+    CK(dalloc(c, c->an_slot, an_slot.size()));
+    CK(h2d(c, c->tile_sp_off, tsp_off));
+    CK(h2d(c, c->tile_an_off, tan_off));
+    CK(h2d(c, c->tile_sp, tsp));
+    CK(h2d(c, c->tile_an, tan));
+    CK(h2d(c, c->tile_an_sslot, sslot));
+    CK(h2d(c, c->sp_slot, sp_slot));
+    CK(h2d(c, c->an_slot, an_slot));
+    c->max_tile_sp = max_sp;
+    c->max_tile_an = max_an;
+    return FN_OK;
+}
+
 int set_block(fn_ctx* c, int block) {
     std::vector<FnTile> t;
     int n = build_tiles(c, block, t);
+    CK(cudaStreamSynchronize(c->stream));
     CK(dalloc(c, c->tiles, t.size()));
     CK(h2d(c, c->tiles, t));
+    int r = build_tile_terms(c, t);
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
     c->ntiles = n;
     c->block = block;
     return FN_OK;
@@ -389,6 +495,15 @@ fn::StepArgs step_args(fn_ctx* c, bool pingpong) {
     A.list_stride = c->list_stride;
     A.list_cap = c->cfg.list_capacity;
     A.counters = c->counters.p;
+    A.tile_sp_off = c->tile_sp_off.p;
+    A.tile_sp = c->tile_sp.p;
+    A.tile_an_off = c->tile_an_off.p;
+    A.tile_an = c->tile_an.p;
+    A.tile_an_sslot = c->tile_an_sslot.p;
+    A.sp_slot = c->sp_slot.p;
+    A.an_slot = c->an_slot.p;
+    A.max_tile_sp = c->max_tile_sp;
+    A.max_tile_an = c->max_tile_an;
     return A;
 }
 
@@ -410,6 +525,7 @@ fn::RebuildArgs rebuild_args(fn_ctx* c) {
     R.list_cap = c->cfg.list_capacity;
     R.cell_cap = c->cfg.cell_capacity;
     R.counters = c->counters.p;
+    R.n_nets = c->n_nets;
     return R;
 }
 
@@ -447,7 +563,10 @@ int launch_one_step(fn_ctx* c, bool do_drift, bool store_v) {
         e1 = next_event(c);
         CK(cudaEventRecord(e0, c->stream));
     }
-    CK(fn::launch_step(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    if (c->tiled)
+        CK(fn::launch_step_tiled(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    else
+        CK(fn::launch_step(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
     if (c->timing) {
         CK(cudaEventRecord(e1, c->stream));
         c->ev_step.emplace_back(e0, e1);
@@ -561,11 +680,27 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         }
         const int npairs = nt * (nt + 1) / 2;
         N.pair_base = (int)c->pairs_h.size();
+        bool any_cut = false, any_hs = false;
         for (int p = 0; p < npairs; ++p) {
             FnPair P;
             pair_coeffs(d.pair_kind[p], d.pair_raw + 4 * p, P);
             c->pairs_h.push_back(P);
+            any_cut |= P.kind == FN_PAIR_LJ || P.kind == FN_PAIR_ST;
+            any_hs |= P.kind == FN_PAIR_HS;
         }
+        /* largest listing radius (squared): cutoff for lj/st, the largest
+           radius + the largest skin for hs (kernel.cl:632-650) */
+        double rmax = 0.0, smax = 0.0;
+        for (int i = 0; i < d.n_beads; ++i) {
+            const float rad = (float)d.radius[i];
+            const float skin = (float)((double)rad + d.settings.skin_ratio);
+            rmax = std::max(rmax, (double)rad);
+            smax = std::max(smax, (double)skin);
+        }
+        c->info[k].any_cut = any_cut;
+        c->info[k].any_hs = any_hs;
+        c->info[k].rmax = rmax;
+        N.list_r2_max = list_r2(c->info[k], N.cutoff_sq, smax);
         NetHost& h = c->info[k];
         h.bead_begin = (int)nb;
         h.bead_end = (int)(nb + d.n_beads);
@@ -696,6 +831,12 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         }
     }
 
+    c->sp_off_h = sp_off;
+    c->sp_ent_h = sp_ent;
+    c->an_off_h = an_off;
+    c->an_ent_h = an_ent;
+    c->an_b_h = an_b;
+    c->an_s_h = an_s;
     c->list_stride = (int)((nb + 31) / 32 * 32);
     const size_t list_n = (size_t)c->list_stride * (size_t)c->cfg.list_capacity;
     for (int k = 0; k < 2; ++k) {
@@ -917,6 +1058,13 @@ FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
     CK(cudaMemcpy(tmp.data(), c->binfo.p, sizeof(int4) * nb, cudaMemcpyDeviceToHost));
     for (long long q = 0; q < nb; ++q) tmp[q].w = float_bits((float)skin[c->perm[q]]);
     CK(cudaMemcpy(c->binfo.p, tmp.data(), sizeof(int4) * nb, cudaMemcpyHostToDevice));
+    for (int k = 0; k < c->n_nets; ++k) {
+        double smax = 0.0;
+        for (int i = c->info[k].bead_begin; i < c->info[k].bead_end; ++i)
+            smax = std::max(smax, (double)(float)skin[i]);
+        c->nets_h[k].list_r2_max = list_r2(c->info[k], c->nets_h[k].cutoff_sq, smax);
+    }
+    CK(cudaMemcpy(c->nets.p, c->nets_h.data(), sizeof(FnNet) * c->n_nets, cudaMemcpyHostToDevice));
     return FN_OK;
 }
 

@@ -236,16 +236,11 @@ __device__ __forceinline__ void drift(const FnNet& N, double minv, float fx, flo
         if (p.x > N.box[0]) p.x = 0.0;
 }
 
-template <bool DAMP, bool DRIFT, bool STORE_V>
-__global__ void __launch_bounds__(512) k_step(const StepArgs A) {
-    const FnTile t = A.tiles[blockIdx.x];
-    const int i = t.begin + (int)threadIdx.x;
-    if (i >= t.end) return;
-    const FnNet& N = A.nets[t.net];
-
-    double4 p = A.pos_in[i];
-    /* base force: damping * v + gravity, then walls (kernel.cl:231-261) */
-    double Fx, Fy, Fz;
+/* Base force of AdvancePosition: damping * v + gravity, then the wall
+   penalty at the drifted position (kernel.cl:231-261). */
+template <bool DAMP>
+__device__ __forceinline__ void base_force(const StepArgs& A, const FnNet& N, int i, double4 p,
+                                           double& Fx, double& Fy, double& Fz) {
     if (DAMP) {
         const float4 v = A.vel[i];
         Fx = N.damping * (double)v.x;
@@ -267,6 +262,66 @@ __global__ void __launch_bounds__(512) k_step(const StepArgs A) {
         if ((N.walls & 2) && p.y > N.box[1]) Fy += (p.y - N.box[1]) * N.wall_k * -1.0;
         if ((N.walls & 1) && p.x > N.box[0]) Fx += (p.x - N.box[0]) * N.wall_k * -1.0;
     }
+}
+
+/* Contacts, AdvanceVelocity and the next step's AdvancePosition for bead i,
+   given its base + bonded force (Fx, Fy, Fz) in FP64. */
+template <bool DAMP, bool DRIFT, bool STORE_V>
+__device__ __forceinline__ void finish_bead(const StepArgs& A, const FnNet& N, int i, double4 p,
+                                            double Fx, double Fy, double Fz) {
+    /* contacts */
+    int n = A.list_count[i];
+    if (n > A.list_cap) n = A.list_cap;
+    const int* __restrict__ lst = A.list + i;
+    for (int k = 0; k < n; ++k) {
+        const int j = lst[(size_t)k * A.list_stride];
+        double Rx, Ry, Rz;
+        if (contact_eval(N, A.pairs, p, A.pos_in[j], Rx, Ry, Rz)) {
+            Fx += Rx;
+            Fy += Ry;
+            Fz += Rz;
+        }
+    }
+
+    const float fx = (float)Fx, fy = (float)Fy, fz = (float)Fz;
+    if (!(isfinite(fx) && isfinite(fy) && isfinite(fz)))
+        atomicAdd(A.counters + FN_CNT_NONFINITE, 1ull);
+
+    /* AdvanceVelocity, kernel.cl:451-462 */
+    double4 im = A.img_in[i];
+    const double minv = im.w;
+    const double half_dt = N.half_dt * minv;
+    const float4 fo = A.force[i];
+    const float4 vo = A.vold[i];
+    double tx = (double)fx, ty = (double)fy, tz = (double)fz;
+    tx += (double)fo.x;
+    ty += (double)fo.y;
+    tz += (double)fo.z;
+    const float vox = (float)(tx * half_dt + (double)vo.x);
+    const float voy = (float)(ty * half_dt + (double)vo.y);
+    const float voz = (float)(tz * half_dt + (double)vo.z);
+    A.force[i] = make_float4(fx, fy, fz, 0.0f);
+    A.vold[i] = make_float4(vox, voy, voz, 0.0f);
+
+    if (DRIFT) {
+        float4 v;
+        drift(N, minv, fx, fy, fz, vox, voy, voz, p, im, v);
+        A.pos_out[i] = p;
+        A.img_out[i] = im;
+        if (DAMP || STORE_V) A.vel[i] = v;
+    }
+}
+
+template <bool DAMP, bool DRIFT, bool STORE_V>
+__global__ void __launch_bounds__(512) k_step(const StepArgs A) {
+    const FnTile t = A.tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    const FnNet& N = A.nets[t.net];
+
+    const double4 p = A.pos_in[i];
+    double Fx, Fy, Fz;
+    base_force<DAMP>(A, N, i, p, Fx, Fy, Fz);
 
     /* springs */
     const int se = A.sp_off[i + 1];
@@ -321,47 +376,106 @@ __global__ void __launch_bounds__(512) k_step(const StepArgs A) {
         }
     }
 
-    /* contacts */
-    int n = A.list_count[i];
-    if (n > A.list_cap) n = A.list_cap;
-    const int* __restrict__ lst = A.list + i;
-    for (int k = 0; k < n; ++k) {
-        const int j = lst[(size_t)k * A.list_stride];
-        double Rx, Ry, Rz;
-        if (contact_eval(N, A.pairs, p, A.pos_in[j], Rx, Ry, Rz)) {
-            Fx += Rx;
-            Fy += Ry;
-            Fz += Rz;
+    finish_bead<DAMP, DRIFT, STORE_V>(A, N, i, p, Fx, Fy, Fz);
+}
+
+/* The same step with the bonded terms evaluated once per tile: the block
+   first evaluates every spring, then every angle incident to its beads into
+   shared memory (flag bits: 1 force acts, 2 broke this step, 4 alive at step
+   start), then each thread gathers its bead's terms from the shared slots in
+   the same order as k_step, so the result is bit-identical to k_step. */
+template <bool DAMP, bool DRIFT, bool STORE_V>
+__global__ void __launch_bounds__(512) k_step_tiled(const StepArgs A) {
+    extern __shared__ double smem[];
+    const int t = blockIdx.x;
+    const FnTile tile = A.tiles[t];
+    double* sp_f = smem;
+    double* an_f = sp_f + 3 * A.max_tile_sp;
+    unsigned char* sp_flag = reinterpret_cast<unsigned char*>(an_f + 6 * A.max_tile_an);
+    unsigned char* an_flag = sp_flag + A.max_tile_sp;
+
+    const int sp0 = A.tile_sp_off[t], nsp = A.tile_sp_off[t + 1] - sp0;
+    for (int q = threadIdx.x; q < nsp; q += blockDim.x) {
+        const int s = A.tile_sp[sp0 + q];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        int broke;
+        const int alive0 = A.sp_status[s] == 1;
+        const int acts = spring_eval(A, s, fx, fy, fz, broke);
+        sp_f[3 * q] = fx;
+        sp_f[3 * q + 1] = fy;
+        sp_f[3 * q + 2] = fz;
+        sp_flag[q] = (unsigned char)(acts | (broke << 1) | (alive0 << 2));
+        if (broke) A.sp_status[s] = 0;
+    }
+    __syncthreads();
+    const int an0 = A.tile_an_off[t], nan = A.tile_an_off[t + 1] - an0;
+    for (int q = threadIdx.x; q < nan; q += blockDim.x) {
+        const int a = A.tile_an[an0 + q];
+        int alive = A.an_status[a] == 1;
+        const int4 b = A.an_b[a];
+        if (alive && b.w == 1) {
+            const int2 ss = A.tile_an_sslot[an0 + q];
+            const unsigned f1 = sp_flag[ss.x], f2 = sp_flag[ss.y];
+            const int ok1 = (f1 & 4) && !(f1 & 2);
+            const int ok2 = (f2 & 4) && !(f2 & 2);
+            if (!ok1 || !ok2) {
+                alive = 0;
+                A.an_status[a] = 0;
+            }
+        }
+        an_flag[q] = (unsigned char)alive;
+        if (alive) {
+            double* o = an_f + 6 * q;
+            angle_eval(A, b, A.an_par[a], o[0], o[1], o[2], o[3], o[4], o[5]);
         }
     }
+    __syncthreads();
 
-    const float fx = (float)Fx, fy = (float)Fy, fz = (float)Fz;
-    if (!(isfinite(fx) && isfinite(fy) && isfinite(fz)))
-        atomicAdd(A.counters + FN_CNT_NONFINITE, 1ull);
-
-    /* AdvanceVelocity, kernel.cl:451-462 */
-    double4 im = A.img_in[i];
-    const double minv = im.w;
-    const double half_dt = N.half_dt * minv;
-    const float4 fo = A.force[i];
-    const float4 vo = A.vold[i];
-    double tx = (double)fx, ty = (double)fy, tz = (double)fz;
-    tx += (double)fo.x;
-    ty += (double)fo.y;
-    tz += (double)fo.z;
-    const float vox = (float)(tx * half_dt + (double)vo.x);
-    const float voy = (float)(ty * half_dt + (double)vo.y);
-    const float voz = (float)(tz * half_dt + (double)vo.z);
-    A.force[i] = make_float4(fx, fy, fz, 0.0f);
-    A.vold[i] = make_float4(vox, voy, voz, 0.0f);
-
-    if (DRIFT) {
-        float4 v;
-        drift(N, minv, fx, fy, fz, vox, voy, voz, p, im, v);
-        A.pos_out[i] = p;
-        A.img_out[i] = im;
-        if (DAMP || STORE_V) A.vel[i] = v;
+    const int i = tile.begin + (int)threadIdx.x;
+    if (i >= tile.end) return;
+    const FnNet& N = A.nets[tile.net];
+    const double4 p = A.pos_in[i];
+    double Fx, Fy, Fz;
+    base_force<DAMP>(A, N, i, p, Fx, Fy, Fz);
+    const int se = A.sp_off[i + 1];
+    for (int e = A.sp_off[i]; e < se; ++e) {
+        const int ent = A.sp_slot[e];
+        const int q = ent >> 1;
+        if (sp_flag[q] & 1) {
+            const double* f = sp_f + 3 * q;
+            if ((ent & 1) == 0) {
+                Fx += f[0];
+                Fy += f[1];
+                Fz += f[2];
+            } else {
+                Fx += f[0] * -1.0;
+                Fy += f[1] * -1.0;
+                Fz += f[2] * -1.0;
+            }
+        }
     }
+    const int ae = A.an_off[i + 1];
+    for (int e = A.an_off[i]; e < ae; ++e) {
+        const int ent = A.an_slot[e];
+        const int q = ent >> 2;
+        const int role = ent & 3;
+        if (!an_flag[q]) continue;
+        const double* o = an_f + 6 * q;
+        if (role == 0) {
+            Fx += o[0];
+            Fy += o[1];
+            Fz += o[2];
+        } else if (role == 2) {
+            Fx += o[3];
+            Fy += o[4];
+            Fz += o[5];
+        } else {
+            Fx += -o[0] - o[3];
+            Fy += -o[1] - o[4];
+            Fz += -o[2] - o[5];
+        }
+    }
+    finish_bead<DAMP, DRIFT, STORE_V>(A, N, i, p, Fx, Fy, Fz);
 }
 
 template <bool STORE_V>
@@ -533,60 +647,98 @@ __device__ __forceinline__ bool list_candidate(const FnNet& N, const FnPair* __r
     return false;
 }
 
+/* Network owning bead i (networks hold consecutive bead ranges). */
+__device__ __forceinline__ int net_of_bead(const FnNet* __restrict__ nets, int n_nets, int i) {
+    int lo = 0, hi = n_nets - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (nets[mid].bead_begin <= i)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+/* Candidates j of one run of consecutive beads in cell order. */
+__device__ __forceinline__ void scan_run(const RebuildArgs& R, const FnNet& N, int i, double4 pi,
+                                         int4 bi, const int* ids, int m, int* __restrict__ out,
+                                         int& n) {
+    for (int k = 0; k < m; ++k) {
+        const int j = ids[k];
+        if (j == i) continue;
+        const double4 pj = R.pos[j];
+        double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+        double length = rx * rx + ry * ry + rz * rz;
+        if (N.list_mi) length = min_image(N, rx, ry, rz, length, N.list_mi);
+        if (!(length < N.list_r2_max)) continue; /* listed by no pair kind */
+        if (list_candidate(N, R.pairs, pi, bi, pj, R.binfo[j])) {
+            if (n < R.list_cap) out[(size_t)n * R.list_stride] = j;
+            ++n;
+        }
+    }
+}
+
 /* Full per-bead lists over the 27-cell neighbourhood (dz, dy, dx ascending,
    beads ascending within a cell): the symmetric closure of the reference's
-   half-shell pair set, in a fixed order. */
-__global__ void k_lists(const RebuildArgs R) {
-    const FnTile t = R.tiles[blockIdx.x];
-    const int i = t.begin + (int)threadIdx.x;
-    if (i >= t.end) return;
+   half-shell pair set, in a fixed order.  Threads walk the beads in cell
+   order, so neighbouring threads share their candidate cells; the three
+   cells of one (dz, dy) row are one contiguous run of the sorted bead array
+   unless the row wraps or a cell overflows. */
+__global__ void k_lists(const RebuildArgs R, long long ncells) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= R.cell_start[ncells]) return; /* beads placed in the grid */
+    const int i = R.cell_beads[t];
     const int c = R.cell_of[i];
+    if (c < 0) return; /* beyond its cell's capacity: listed nowhere */
+    const FnNet& N = R.nets[net_of_bead(R.nets, R.n_nets, i)];
+    const double4 pi = R.pos[i];
+    const int4 bi = R.binfo[i];
+    const int lc = c - N.cell_base;
+    const int cz = lc / N.nxy;
+    const int cy = (lc - cz * N.nxy) / N.nx;
+    const int cx = lc - cz * N.nxy - cy * N.nx;
+    int* __restrict__ out = R.list + i;
     int n = 0;
-    if (c >= 0) {
-        const FnNet& N = R.nets[t.net];
-        const double4 pi = R.pos[i];
-        const int4 bi = R.binfo[i];
-        const int lc = c - N.cell_base;
-        const int cz = lc / N.nxy;
-        const int cy = (lc - cz * N.nxy) / N.nx;
-        const int cx = lc - cz * N.nxy - cy * N.nx;
-        int* __restrict__ out = R.list + i;
-        for (int dz = -1; dz <= 1; ++dz) {
-            int z = cz + dz;
-            if (z < 0 || z >= N.nz) {
-                if (!(N.periodic & 4)) continue;
-                z = z < 0 ? N.nz - 1 : 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+        int z = cz + dz;
+        if (z < 0 || z >= N.nz) {
+            if (!(N.periodic & 4)) continue;
+            z = z < 0 ? N.nz - 1 : 0;
+        }
+        for (int dy = -1; dy <= 1; ++dy) {
+            int y = cy + dy;
+            if (y < 0 || y >= N.ny) {
+                if (!(N.periodic & 2)) continue;
+                y = y < 0 ? N.ny - 1 : 0;
             }
-            for (int dy = -1; dy <= 1; ++dy) {
-                int y = cy + dy;
-                if (y < 0 || y >= N.ny) {
-                    if (!(N.periodic & 2)) continue;
-                    y = y < 0 ? N.ny - 1 : 0;
+            const int row = N.cell_base + y * N.nx + z * N.nxy;
+            if (cx >= 1 && cx + 1 < N.nx) {
+                const int c0 = row + cx - 1;
+                const int s0 = R.cell_start[c0];
+                const int s3 = R.cell_start[c0 + 3];
+                if (s3 - s0 <= R.cell_cap ||
+                    (R.cell_count[c0] <= R.cell_cap && R.cell_count[c0 + 1] <= R.cell_cap &&
+                     R.cell_count[c0 + 2] <= R.cell_cap)) {
+                    scan_run(R, N, i, pi, bi, R.cell_beads + s0, s3 - s0, out, n);
+                    continue;
                 }
-                for (int dx = -1; dx <= 1; ++dx) {
-                    int x = cx + dx;
-                    if (x < 0 || x >= N.nx) {
-                        if (!(N.periodic & 1)) continue;
-                        x = x < 0 ? N.nx - 1 : 0;
-                    }
-                    const int nc = N.cell_base + x + y * N.nx + z * N.nxy;
-                    int m = R.cell_count[nc];
-                    if (m > R.cell_cap) m = R.cell_cap;
-                    const int* ids = R.cell_beads + R.cell_start[nc];
-                    for (int k = 0; k < m; ++k) {
-                        const int j = ids[k];
-                        if (j == i) continue;
-                        if (list_candidate(N, R.pairs, pi, bi, R.pos[j], R.binfo[j])) {
-                            if (n < R.list_cap) out[(size_t)n * R.list_stride] = j;
-                            ++n;
-                        }
-                    }
+            }
+            for (int dx = -1; dx <= 1; ++dx) {
+                int x = cx + dx;
+                if (x < 0 || x >= N.nx) {
+                    if (!(N.periodic & 1)) continue;
+                    x = x < 0 ? N.nx - 1 : 0;
                 }
+                const int nc = row + x;
+                int m = R.cell_count[nc];
+                if (m > R.cell_cap) m = R.cell_cap;
+                scan_run(R, N, i, pi, bi, R.cell_beads + R.cell_start[nc], m, out, n);
             }
         }
-        if (n > R.list_cap)
-            atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
     }
+    if (n > R.list_cap)
+        atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
     R.list_count[i] = n;
 }
 
@@ -756,6 +908,43 @@ cudaError_t launch_step(const StepArgs& A, int ntiles, int block, bool damp, boo
     return cudaGetLastError();
 }
 
+template <bool DAMP, bool DRIFT, bool STORE_V>
+static cudaError_t set_tiled_smem(size_t bytes) {
+    return cudaFuncSetAttribute(k_step_tiled<DAMP, DRIFT, STORE_V>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t prepare_step_tiled(size_t bytes) {
+    cudaError_t e;
+    if ((e = set_tiled_smem<true, true, true>(bytes))) return e;
+    if ((e = set_tiled_smem<true, false, false>(bytes))) return e;
+    if ((e = set_tiled_smem<false, true, true>(bytes))) return e;
+    if ((e = set_tiled_smem<false, true, false>(bytes))) return e;
+    return set_tiled_smem<false, false, false>(bytes);
+}
+
+cudaError_t launch_step_tiled(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
+                              bool store_v, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    const size_t sm = step_tiled_smem(A.max_tile_sp, A.max_tile_an);
+    if (damp) {
+        if (do_drift)
+            k_step_tiled<true, true, true><<<ntiles, block, sm, s>>>(A);
+        else
+            k_step_tiled<true, false, false><<<ntiles, block, sm, s>>>(A);
+    } else {
+        if (do_drift) {
+            if (store_v)
+                k_step_tiled<false, true, true><<<ntiles, block, sm, s>>>(A);
+            else
+                k_step_tiled<false, true, false><<<ntiles, block, sm, s>>>(A);
+        } else {
+            k_step_tiled<false, false, false><<<ntiles, block, sm, s>>>(A);
+        }
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_drift(const StepArgs& A, int ntiles, int block, bool store_v, cudaStream_t s) {
     if (ntiles <= 0) return cudaSuccess;
     if (store_v)
@@ -793,7 +982,9 @@ cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, 
                                                           R.cell_start);
     if (nb > 0) k_scatter<<<(nb + 255) / 256, 256, 0, s>>>(R, nb);
     k_cell_sort<<<(unsigned)((ncells + 255) / 256), 256, 0, s>>>(R, (int)ncells);
-    if (ntiles > 0) k_lists<<<ntiles, block, 0, s>>>(R);
+    if ((e = cudaMemsetAsync(R.list_count, 0, sizeof(int) * (size_t)nb, s))) return e;
+    /* every bead may sit in the grid; threads past the grid total return */
+    if (nb > 0) k_lists<<<(nb + 127) / 128, 128, 0, s>>>(R, ncells);
     return cudaGetLastError();
 }
 

@@ -43,7 +43,24 @@ struct StepArgs {
     int list_stride;
     int list_cap;
     unsigned long long* counters;
+    /* per-tile bonded terms (tiled step kernel): each tile evaluates the
+       springs / angles incident to its beads once, into shared memory */
+    const int* tile_sp_off;    /* ntiles + 1 */
+    const int* tile_sp;        /* spring ids of each tile, ascending */
+    const int* tile_an_off;    /* ntiles + 1 */
+    const int* tile_an;        /* angle ids of each tile, ascending */
+    const int2* tile_an_sslot; /* per tile angle: slots of s1, s2 (HR_FL) or -1 */
+    const int* sp_slot;        /* per bead entry: tile spring slot << 1 | role */
+    const int* an_slot;        /* per bead entry: tile angle slot << 2 | role */
+    int max_tile_sp;
+    int max_tile_an;
 };
+
+/* dynamic shared memory of the tiled step kernel */
+inline size_t step_tiled_smem(int max_sp, int max_an) {
+    return sizeof(double) * 3 * (size_t)max_sp + sizeof(double) * 6 * (size_t)max_an +
+           (size_t)max_sp + (size_t)max_an + 16;
+}
 
 struct RebuildArgs {
     const FnTile* tiles;
@@ -62,6 +79,7 @@ struct RebuildArgs {
     int list_cap;
     int cell_cap;
     unsigned long long* counters;
+    int n_nets;
 };
 
 struct ObserveArgs {
@@ -78,6 +96,9 @@ struct ObserveArgs {
 
 cudaError_t launch_step(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
                         bool store_v, cudaStream_t s);
+cudaError_t launch_step_tiled(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
+                              bool store_v, cudaStream_t s);
+cudaError_t prepare_step_tiled(size_t smem_bytes);
 cudaError_t launch_drift(const StepArgs& A, int ntiles, int block, bool store_v, cudaStream_t s);
 cudaError_t launch_forces_only(const StepArgs& A, int ntiles, int block, int terms, cudaStream_t s);
 cudaError_t launch_reset_energy(float4* force, float4* vel, float4* vold, int n, cudaStream_t s);

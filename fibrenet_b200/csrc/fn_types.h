@@ -34,6 +34,7 @@ struct FnNet {
     int pair_base;   /* first entry of this network in the pair table */
     int bead_begin, bead_end;
     int pad_;
+    double list_r2_max; /* no pair further apart than this (squared) is listed */
 };
 
 /* Pair coefficients c1..c6 (SimulationManager.cpp:891-932) and kind. */
