@@ -106,6 +106,13 @@ struct fn_ctx {
     DevBuf<int2> tile_an_sslot;
     int max_tile_sp = 0, max_tile_an = 0;
     bool tiled = false;
+    /* chain form */
+    bool chain = false;
+    std::vector<int> sp_bead, an_bead; /* spring -> lower bead, angle -> centre bead */
+    std::vector<unsigned char> ch_flags_h;
+    DevBuf<float4> ch_sp;
+    DevBuf<float2> ch_an;
+    DevBuf<unsigned char> ch_flags, ch_status;
     DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
     DevBuf<int> scan_sums;
     DevBuf<FnTile> tiles;
@@ -191,6 +198,10 @@ void free_all(fn_ctx* c) {
     dfree(c, c->an_s);
     dfree(c, c->an_par);
     dfree(c, c->an_status);
+    dfree(c, c->ch_sp);
+    dfree(c, c->ch_an);
+    dfree(c, c->ch_flags);
+    dfree(c, c->ch_status);
     dfree(c, c->tile_sp_off);
     dfree(c, c->tile_sp);
     dfree(c, c->tile_an_off);
@@ -452,14 +463,94 @@ int build_tile_terms(fn_ctx* c, const std::vector<FnTile>& tiles) {
     return FN_OK;
 }
 
+/* Chain form: every spring joins beads j, j+1 (one spring per j), every
+   angle is (j-1, j, j+1) or (j+1, j, j-1) (one per centre), HR_FL angles use
+   exactly the two springs around their centre, and around every bead the
+   incident springs and angles appear in ascending index in the order
+   previous, next (springs) and centre j-1, j, j+1 (angles), which is the
+   incidence path's order.  Builds the per-bead records when it holds. */
+bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<signed char>& sp_type,
+                 const std::vector<int4>& an_b, const std::vector<int2>& an_s) {
+    using namespace fn;
+    const long long nb = c->nb;
+    std::vector<int> next_sp(nb, -1), centre_an(nb, -1);
+    std::vector<unsigned char> fl(nb, 0);
+    for (long long s = 0; s < c->ns; ++s) {
+        const int a = sp_ends[s].x, b = sp_ends[s].y;
+        const int lo = std::min(a, b), hi = std::max(a, b);
+        if (hi != lo + 1 || next_sp[lo] != -1) return false;
+        next_sp[lo] = (int)s;
+        fl[lo] |= FN_CH_SPRING;
+        if (a == hi) fl[lo] |= FN_CH_SP_REV;
+        if (sp_type[s] == 1)
+            fl[lo] |= FN_CH_SP_FL;
+        else if (sp_type[s] != 0)
+            fl[lo] |= FN_CH_SP_INERT;
+    }
+    for (long long a = 0; a < c->na; ++a) {
+        const int4 b = an_b[a];
+        const bool fwd = b.x == b.y - 1 && b.z == b.y + 1;
+        const bool rev = b.x == b.y + 1 && b.z == b.y - 1;
+        if (!(fwd || rev) || centre_an[b.y] != -1) return false;
+        centre_an[b.y] = (int)a;
+        fl[b.y] |= FN_CH_ANGLE;
+        if (rev) fl[b.y] |= FN_CH_AN_REV;
+        if (b.w == 1) {
+            fl[b.y] |= FN_CH_AN_FL;
+            const int sp = next_sp[b.y - 1], sn = next_sp[b.y];
+            const int2 ss = an_s[a];
+            if (sp < 0 || sn < 0) return false;
+            if (!((ss.x == sp && ss.y == sn) || (ss.x == sn && ss.y == sp))) return false;
+        }
+    }
+    for (long long i = 0; i < nb; ++i) {
+        if (i > 0 && next_sp[i - 1] >= 0 && next_sp[i] >= 0 && next_sp[i - 1] > next_sp[i]) return false;
+        int last = -1;
+        for (long long q = i - 1; q <= i + 1; ++q) {
+            if (q < 0 || q >= nb || centre_an[q] < 0) continue;
+            if (centre_an[q] < last) return false;
+            last = centre_an[q];
+        }
+    }
+    std::vector<float4> chs(nb, make_float4(0, 0, 0, 0));
+    std::vector<float2> cha(nb, make_float2(0, 0));
+    std::vector<unsigned char> st(nb, 0);
+    c->sp_bead.assign(c->ns, 0);
+    c->an_bead.assign(c->na, 0);
+    for (long long i = 0; i < nb; ++i) {
+        if (next_sp[i] >= 0) {
+            chs[i] = c->sp_par_h[next_sp[i]];
+            c->sp_bead[next_sp[i]] = (int)i;
+            st[i] |= 1;
+        }
+        if (centre_an[i] >= 0) {
+            cha[i] = c->an_par_h[centre_an[i]];
+            c->an_bead[centre_an[i]] = (int)i;
+            st[i] |= 2;
+        }
+    }
+    if (dalloc(c, c->ch_sp, nb) || dalloc(c, c->ch_an, nb) || dalloc(c, c->ch_flags, nb) ||
+        dalloc(c, c->ch_status, nb))
+        return false;
+    if (h2d(c, c->ch_sp, chs) || h2d(c, c->ch_an, cha) || h2d(c, c->ch_flags, fl) ||
+        h2d(c, c->ch_status, st))
+        return false;
+    c->ch_flags_h = fl;
+    return true;
+}
+
 int set_block(fn_ctx* c, int block) {
     std::vector<FnTile> t;
     int n = build_tiles(c, block, t);
     CK(cudaStreamSynchronize(c->stream));
     CK(dalloc(c, c->tiles, t.size()));
     CK(h2d(c, c->tiles, t));
-    int r = build_tile_terms(c, t);
-    if (r) return r;
+    if (c->chain) {
+        CK(fn::prepare_step_chain(fn::step_chain_smem(block)));
+    } else {
+        int r = build_tile_terms(c, t);
+        if (r) return r;
+    }
     CK(cudaStreamSynchronize(c->stream));
     c->ntiles = n;
     c->block = block;
@@ -504,6 +595,11 @@ fn::StepArgs step_args(fn_ctx* c, bool pingpong) {
     A.an_slot = c->an_slot.p;
     A.max_tile_sp = c->max_tile_sp;
     A.max_tile_an = c->max_tile_an;
+    A.ch_sp = c->ch_sp.p;
+    A.ch_an = c->ch_an.p;
+    A.ch_flags = c->ch_flags.p;
+    A.ch_status = c->ch_status.p;
+    A.nb = (int)c->nb;
     return A;
 }
 
@@ -563,7 +659,9 @@ int launch_one_step(fn_ctx* c, bool do_drift, bool store_v) {
         e1 = next_event(c);
         CK(cudaEventRecord(e0, c->stream));
     }
-    if (c->tiled)
+    if (c->chain)
+        CK(fn::launch_step_chain(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    else if (c->tiled)
         CK(fn::launch_step_tiled(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
     else
         CK(fn::launch_step(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
@@ -900,6 +998,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     CK(cudaMemsetAsync(c->list_count.p, 0, sizeof(int) * (size_t)nb, c->stream));
     CK(cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
     CK(cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
+    c->chain = c->cfg.chain_mode != 2 && build_chain(c, sp_ends, sp_type, an_b, an_s);
     int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128);
     if (r) return r;
     CK(cudaStreamSynchronize(c->stream));
@@ -1083,6 +1182,11 @@ FN_API int fn_set_springs(fn_ctx* c, const double* rest, const double* k, const 
     }
     if (c->ns > 0)
         CK(cudaMemcpy(c->sp_par.p, c->sp_par_h.data(), sizeof(float4) * c->ns, cudaMemcpyHostToDevice));
+    if (c->chain && c->ns > 0) {
+        std::vector<float4> chs(c->nb, make_float4(0, 0, 0, 0));
+        for (long long q = 0; q < c->ns; ++q) chs[c->sp_bead[q]] = c->sp_par_h[q];
+        CK(cudaMemcpy(c->ch_sp.p, chs.data(), sizeof(float4) * c->nb, cudaMemcpyHostToDevice));
+    }
     return FN_OK;
 }
 
@@ -1097,6 +1201,11 @@ FN_API int fn_set_angles(fn_ctx* c, const double* theta0, const double* k) {
     }
     if (c->na > 0)
         CK(cudaMemcpy(c->an_par.p, c->an_par_h.data(), sizeof(float2) * c->na, cudaMemcpyHostToDevice));
+    if (c->chain && c->na > 0) {
+        std::vector<float2> cha(c->nb, make_float2(0, 0));
+        for (long long q = 0; q < c->na; ++q) cha[c->an_bead[q]] = c->an_par_h[q];
+        CK(cudaMemcpy(c->ch_an.p, cha.data(), sizeof(float2) * c->nb, cudaMemcpyHostToDevice));
+    }
     return FN_OK;
 }
 
@@ -1104,6 +1213,16 @@ FN_API int fn_download_status(fn_ctx* c, int* spring_status, int* angle_status) 
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
+    if (c->chain) {
+        std::vector<unsigned char> st(c->nb);
+        CK(cudaMemcpyAsync(st.data(), c->ch_status.p, c->nb, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (spring_status)
+            for (long long q = 0; q < c->ns; ++q) spring_status[q] = st[c->sp_bead[q]] & 1;
+        if (angle_status)
+            for (long long q = 0; q < c->na; ++q) angle_status[q] = (st[c->an_bead[q]] >> 1) & 1;
+        return FN_OK;
+    }
     std::vector<signed char> s(c->ns), a(c->na);
     if (c->ns > 0 && spring_status)
         CK(cudaMemcpyAsync(s.data(), c->sp_status.p, c->ns, cudaMemcpyDeviceToHost, c->stream));
@@ -1122,6 +1241,18 @@ FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_s
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->chain) {
+        std::vector<unsigned char> st(c->nb);
+        CK(cudaMemcpy(st.data(), c->ch_status.p, c->nb, cudaMemcpyDeviceToHost));
+        if (spring_status)
+            for (long long q = 0; q < c->ns; ++q)
+                st[c->sp_bead[q]] = (unsigned char)((st[c->sp_bead[q]] & ~1u) | (spring_status[q] == 1 ? 1u : 0u));
+        if (angle_status)
+            for (long long q = 0; q < c->na; ++q)
+                st[c->an_bead[q]] = (unsigned char)((st[c->an_bead[q]] & ~2u) | (angle_status[q] == 1 ? 2u : 0u));
+        CK(cudaMemcpy(c->ch_status.p, st.data(), c->nb, cudaMemcpyHostToDevice));
+        return FN_OK;
+    }
     if (spring_status && c->ns > 0) {
         std::vector<signed char> s(c->ns);
         for (long long q = 0; q < c->ns; ++q) s[q] = (signed char)spring_status[q];
@@ -1142,6 +1273,8 @@ FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out
     CK(cudaSetDevice(c->cfg.device));
     const NetHost& h = c->info[net];
     fn::ObserveArgs O{};
+    O.ch_flags = c->chain ? c->ch_flags.p : nullptr;
+    O.ch_status = c->chain ? c->ch_status.p : nullptr;
     O.pos = c->pos[c->cur].p;
     O.force = c->force.p;
     O.sp_status = c->sp_status.p;
@@ -1171,6 +1304,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     if (!c || !out) return FN_ERR_ARG;
     std::memset(out, 0, sizeof *out);
     out->block_size = c->block;
+    out->bond_path = c->chain ? 2 : (c->tiled ? 1 : 0);
     out->n_networks = c->n_nets;
     out->n_beads = c->nb;
     out->device_bytes = c->device_bytes;
@@ -1290,7 +1424,10 @@ FN_API int fn_forces_only(fn_ctx* c, int terms) {
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
     fn::StepArgs A = step_args(c, false);
-    CK(fn::launch_forces_only(A, c->ntiles, c->block, terms, c->stream));
+    if (c->chain)
+        CK(fn::launch_forces_chain(A, c->ntiles, c->block, terms, c->stream));
+    else
+        CK(fn::launch_forces_only(A, c->ntiles, c->block, terms, c->stream));
     return FN_OK;
 }
 

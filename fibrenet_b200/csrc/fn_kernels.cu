@@ -38,6 +38,10 @@ __device__ __forceinline__ int getadress(int t1, int t2, int size) {
                      : ((size * t2) + t1 - ((t2 * (t2 + 1)) / 2));
 }
 
+__device__ __forceinline__ int spring_pts(double ax, double ay, double az, double bx, double by,
+                                          double bz, float4 par, int type, double& fx, double& fy,
+                                          double& fz, int& broke);
+
 /* Spring s (kernel.cl:371-437): returns 1 when a force acts, f = force on p1
    (p2 takes f * -1.0); broke = 1 when this evaluation breaks an HR_FL
    spring (kernel.cl:391-397). */
@@ -50,8 +54,16 @@ __device__ __forceinline__ int spring_eval(const StepArgs& A, int s, double& fx,
     const int2 e = A.sp_ends[s];
     const double4 a = A.img_in[e.x];
     const double4 b = A.img_in[e.y];
-    const float4 par = A.sp_par[s];
-    double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    return spring_pts(a.x, a.y, a.z, b.x, b.y, b.z, A.sp_par[s], type, fx, fy, fz, broke);
+}
+
+/* The spring force of kernel.cl:377-424 from the image positions of p1 (a)
+   and p2 (b); shared by the incidence and chain kernels. */
+__device__ __forceinline__ int spring_pts(double ax, double ay, double az, double bx, double by,
+                                          double bz, float4 par, int type, double& fx, double& fy,
+                                          double& fz, int& broke) {
+    broke = 0;
+    double dx = ax - bx, dy = ay - by, dz = az - bz;
     double l = sqrt(dx * dx + dy * dy + dz * dz);
     double factor = (double)par.x - l;
     if (l != 0.0) l = 1.0 / l;
@@ -80,15 +92,14 @@ __device__ __forceinline__ int spring_alive_after(const StepArgs& A, int s) {
     return !broke;
 }
 
-/* Angle force (kernel.cl:291-348): pa acts on b1, pc on b3. */
-__device__ __forceinline__ void angle_eval(const StepArgs& A, int4 b, float2 par, double& pax,
-                                           double& pay, double& paz, double& pcx, double& pcy,
-                                           double& pcz) {
-    const double4 t2 = A.img_in[b.y];
-    const double4 t1 = A.img_in[b.x];
-    const double4 t3 = A.img_in[b.z];
-    const double bax = t1.x - t2.x, bay = t1.y - t2.y, baz = t1.z - t2.z;
-    const double bcx = t3.x - t2.x, bcy = t3.y - t2.y, bcz = t3.z - t2.z;
+/* Angle force (kernel.cl:291-348) from the image positions of b1 (t1),
+   b2 (t2), b3 (t3): pa acts on b1, pc on b3. */
+__device__ __forceinline__ void angle_pts(double t1x, double t1y, double t1z, double t2x,
+                                          double t2y, double t2z, double t3x, double t3y,
+                                          double t3z, float2 par, double& pax, double& pay,
+                                          double& paz, double& pcx, double& pcy, double& pcz) {
+    const double bax = t1x - t2x, bay = t1y - t2y, baz = t1z - t2z;
+    const double bcx = t3x - t2x, bcy = t3y - t2y, bcz = t3z - t2z;
     const double cbx = bcx * -1.0, cby = bcy * -1.0, cbz = bcz * -1.0;
     const double l_ba = sqrt(bax * bax + bay * bay + baz * baz);
     const double l_bc = sqrt(bcx * bcx + bcy * bcy + bcz * bcz);
@@ -120,6 +131,16 @@ __device__ __forceinline__ void angle_eval(const StepArgs& A, int4 b, float2 par
     pcx *= ln;
     pcy *= ln;
     pcz *= ln;
+}
+
+__device__ __forceinline__ void angle_eval(const StepArgs& A, int4 b, float2 par, double& pax,
+                                           double& pay, double& paz, double& pcx, double& pcy,
+                                           double& pcz) {
+    const double4 t2 = A.img_in[b.y];
+    const double4 t1 = A.img_in[b.x];
+    const double4 t3 = A.img_in[b.z];
+    angle_pts(t1.x, t1.y, t1.z, t2.x, t2.y, t2.z, t3.x, t3.y, t3.z, par, pax, pay, paz, pcx, pcy,
+              pcz);
 }
 
 /* Minimum image on the axes of mask (kernel.cl:598-627, 844-870). */
@@ -267,6 +288,10 @@ __device__ __forceinline__ void base_force(const StepArgs& A, const FnNet& N, in
 /* Contacts, AdvanceVelocity and the next step's AdvancePosition for bead i,
    given its base + bonded force (Fx, Fy, Fz) in FP64. */
 template <bool DAMP, bool DRIFT, bool STORE_V>
+__device__ __forceinline__ void kick_drift_store(const StepArgs& A, const FnNet& N, int i,
+                                                 double4 p, double Fx, double Fy, double Fz);
+
+template <bool DAMP, bool DRIFT, bool STORE_V>
 __device__ __forceinline__ void finish_bead(const StepArgs& A, const FnNet& N, int i, double4 p,
                                             double Fx, double Fy, double Fz) {
     /* contacts */
@@ -282,7 +307,14 @@ __device__ __forceinline__ void finish_bead(const StepArgs& A, const FnNet& N, i
             Fz += Rz;
         }
     }
+    kick_drift_store<DAMP, DRIFT, STORE_V>(A, N, i, p, Fx, Fy, Fz);
+}
 
+/* AdvanceVelocity and the next AdvancePosition for bead i with its complete
+   force (Fx, Fy, Fz), then the stores. */
+template <bool DAMP, bool DRIFT, bool STORE_V>
+__device__ __forceinline__ void kick_drift_store(const StepArgs& A, const FnNet& N, int i,
+                                                 double4 p, double Fx, double Fy, double Fz) {
     const float fx = (float)Fx, fy = (float)Fy, fz = (float)Fz;
     if (!(isfinite(fx) && isfinite(fy) && isfinite(fz)))
         atomicAdd(A.counters + FN_CNT_NONFINITE, 1ull);
@@ -478,6 +510,261 @@ __global__ void __launch_bounds__(512) k_step_tiled(const StepArgs A) {
     finish_bead<DAMP, DRIFT, STORE_V>(A, N, i, p, Fx, Fy, Fz);
 }
 
+/* Exclusive prefix sum of v over the block (any size up to 1024); total
+   receives the block sum.  warp_sums needs 33 ints. */
+__device__ __forceinline__ int block_scan_any(int v, int* warp_sums, int& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < nwarps ? warp_sums[lane] : 0;
+        int sacc = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, sacc, o);
+            if (lane >= o) sacc += y;
+        }
+        warp_sums[lane] = sacc - w;
+        if (lane == 31) warp_sums[32] = sacc;
+    }
+    __syncthreads();
+    total = warp_sums[32];
+    const int r = x - v + warp_sums[warp];
+    __syncthreads();
+    return r;
+}
+
+/* Step kernel for networks in chain form (every spring joins consecutive
+   beads j, j+1 and every angle is centred on its middle bead, as fibres
+   are).  The block stages the image positions of its beads plus two halo
+   beads on each side in shared memory, evaluates every spring and angle
+   touching its beads once (springs first: an HR_FL angle dies with either of
+   its springs in the same step, kernel.cl:274-286), then each thread adds its
+   bead's terms in ascending bond order -- previous spring, next spring,
+   angles centred on j-1, j, j+1 -- which is the order of the incidence path,
+   so both produce identical bits.  Statuses are written back by the owning
+   thread.  FORCES_ONLY evaluates the selected terms alone (no base force, no
+   kick or drift, no status change). */
+template <bool DAMP, bool DRIFT, bool STORE_V, bool FORCES_ONLY>
+__global__ void __launch_bounds__(512) k_step_chain(const StepArgs A, int terms) {
+    extern __shared__ __align__(32) unsigned char smem_raw[];
+    const FnTile tile = A.tiles[blockIdx.x];
+    const int b0 = tile.begin, n = tile.end - tile.begin;
+    const ChainSmem L = chain_smem_layout(blockDim.x);
+    double* s_img = reinterpret_cast<double*>(smem_raw + L.img);  /* slot u <-> bead b0 - 2 + u */
+    double* s_spf = reinterpret_cast<double*>(smem_raw + L.spf);  /* lower bead b0 - 2 + u */
+    double* s_ang = reinterpret_cast<double*>(smem_raw + L.ang);  /* centre bead b0 - 1 + u */
+    unsigned char* s_flag = smem_raw + L.flag;
+    unsigned char* s_stat = smem_raw + L.stat;
+    unsigned char* s_tsp = smem_raw + L.tsp; /* spring term: 1 acts, 2 broke, 4 alive at start */
+    unsigned char* s_tan = smem_raw + L.tan; /* angle term alive */
+    const int tid = threadIdx.x;
+
+    for (int u = tid; u < n + 4; u += blockDim.x) {
+        const int j = b0 - 2 + u;
+        unsigned char fl = 0, st = 0;
+        if (j >= 0 && j < A.nb) {
+            const double4 q = A.img_in[j];
+            s_img[3 * u] = q.x;
+            s_img[3 * u + 1] = q.y;
+            s_img[3 * u + 2] = q.z;
+            fl = A.ch_flags[j];
+            st = A.ch_status[j];
+        }
+        s_flag[u] = fl;
+        s_stat[u] = st;
+    }
+    __syncthreads();
+
+    const bool want_sp = !FORCES_ONLY || (terms & 1);
+    const bool want_an = !FORCES_ONLY || (terms & 2);
+    for (int u = tid; u < n + 3; u += blockDim.x) {
+        const unsigned fl = s_flag[u];
+        unsigned char tf = 0;
+        if (fl & FN_CH_SPRING) {
+            const int alive0 = s_stat[u] & 1;
+            tf = (unsigned char)(alive0 << 2);
+            if (alive0 && !(fl & FN_CH_SP_INERT)) {
+                const int j = b0 - 2 + u;
+                const float4 par = A.ch_sp[j];
+                const double* a = s_img + 3 * ((fl & FN_CH_SP_REV) ? u + 1 : u);
+                const double* b = s_img + 3 * ((fl & FN_CH_SP_REV) ? u : u + 1);
+                double fx = 0.0, fy = 0.0, fz = 0.0;
+                int broke;
+                const int acts = spring_pts(a[0], a[1], a[2], b[0], b[1], b[2], par,
+                                            (fl & FN_CH_SP_FL) ? 1 : 0, fx, fy, fz, broke);
+                s_spf[3 * u] = fx;
+                s_spf[3 * u + 1] = fy;
+                s_spf[3 * u + 2] = fz;
+                tf |= (unsigned char)(acts | (broke << 1));
+            }
+        }
+        s_tsp[u] = tf;
+    }
+    __syncthreads();
+
+    for (int u = tid; u < n + 2; u += blockDim.x) {
+        const unsigned fl = s_flag[u + 1];
+        int alive = (fl & FN_CH_ANGLE) && (s_stat[u + 1] & 2);
+        if (alive && (fl & FN_CH_AN_FL)) {
+            const unsigned f1 = s_tsp[u], f2 = s_tsp[u + 1];
+            if (!((f1 & 4) && !(f1 & 2)) || !((f2 & 4) && !(f2 & 2))) alive = 0;
+        }
+        s_tan[u] = (unsigned char)alive;
+        if (alive && want_an) {
+            const int j = b0 - 1 + u;
+            const double* t1 = s_img + 3 * ((fl & FN_CH_AN_REV) ? u + 2 : u);
+            const double* t2 = s_img + 3 * (u + 1);
+            const double* t3 = s_img + 3 * ((fl & FN_CH_AN_REV) ? u : u + 2);
+            double* o = s_ang + 6 * u;
+            angle_pts(t1[0], t1[1], t1[2], t2[0], t2[1], t2[2], t3[0], t3[1], t3[2], A.ch_an[j],
+                      o[0], o[1], o[2], o[3], o[4], o[5]);
+        }
+    }
+    __syncthreads();
+
+    const bool active = tid < n;
+    const int i = b0 + tid;
+    const FnNet& N = A.nets[tile.net];
+    double4 p = make_double4(0.0, 0.0, 0.0, 0.0);
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    int nc = 0;
+    if (active) {
+        p = A.pos_in[i];
+        if (!FORCES_ONLY) base_force<DAMP>(A, N, i, p, Fx, Fy, Fz);
+        if (want_sp) {
+            /* spring (i-1, i): bead i is p1 when the spring is reversed */
+            const unsigned fp = s_flag[tid + 1];
+            if ((fp & FN_CH_SPRING) && (s_tsp[tid + 1] & 1)) {
+                const double* f = s_spf + 3 * (tid + 1);
+                if (fp & FN_CH_SP_REV) {
+                    Fx += f[0];
+                    Fy += f[1];
+                    Fz += f[2];
+                } else {
+                    Fx += f[0] * -1.0;
+                    Fy += f[1] * -1.0;
+                    Fz += f[2] * -1.0;
+                }
+            }
+            /* spring (i, i+1): bead i is p1 unless reversed */
+            const unsigned fn = s_flag[tid + 2];
+            if ((fn & FN_CH_SPRING) && (s_tsp[tid + 2] & 1)) {
+                const double* f = s_spf + 3 * (tid + 2);
+                if (fn & FN_CH_SP_REV) {
+                    Fx += f[0] * -1.0;
+                    Fy += f[1] * -1.0;
+                    Fz += f[2] * -1.0;
+                } else {
+                    Fx += f[0];
+                    Fy += f[1];
+                    Fz += f[2];
+                }
+            }
+        }
+        if (want_an) {
+            /* centred on i-1: bead i is b3, or b1 when reversed */
+            if (s_tan[tid]) {
+                const double* o = s_ang + 6 * tid;
+                const int k = (s_flag[tid + 1] & FN_CH_AN_REV) ? 0 : 3;
+                Fx += o[k];
+                Fy += o[k + 1];
+                Fz += o[k + 2];
+            }
+            /* centred on i: bead i is b2 */
+            if (s_tan[tid + 1]) {
+                const double* o = s_ang + 6 * (tid + 1);
+                Fx += -o[0] - o[3];
+                Fy += -o[1] - o[4];
+                Fz += -o[2] - o[5];
+            }
+            /* centred on i+1: bead i is b1, or b3 when reversed */
+            if (s_tan[tid + 2]) {
+                const double* o = s_ang + 6 * (tid + 2);
+                const int k = (s_flag[tid + 3] & FN_CH_AN_REV) ? 3 : 0;
+                Fx += o[k];
+                Fy += o[k + 1];
+                Fz += o[k + 2];
+            }
+        }
+        if (!FORCES_ONLY || (terms & 4)) {
+            nc = A.list_count[i];
+            if (nc > A.list_cap) nc = A.list_cap;
+        }
+    }
+
+    /* contacts, load-balanced over the block: item w of the block's
+       concatenated lists is evaluated by thread w mod blockDim, the results
+       land in shared memory, and each bead adds its own items in list order
+       (the order of the sequential loop, so the sums are identical) */
+    double4* s_pos = reinterpret_cast<double4*>(smem_raw + L.pos);
+    int* s_off = reinterpret_cast<int*>(smem_raw + L.off);
+    int* s_ws = reinterpret_cast<int*>(smem_raw + L.ws);
+    double* s_R = reinterpret_cast<double*>(smem_raw + L.res);
+    unsigned char* s_Rf = smem_raw + L.resf;
+    const int chunk = 2 * blockDim.x;
+    if (active) s_pos[tid] = p;
+    int total;
+    const int off = block_scan_any(nc, s_ws, total);
+    s_off[tid] = off;
+    if (tid == 0) s_off[blockDim.x] = total;
+    __syncthreads();
+    for (int base = 0; base < total; base += chunk) {
+        const int lim = min(base + chunk, total);
+        for (int w = base + tid; w < lim; w += blockDim.x) {
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_off[mid] <= w)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const int k = w - s_off[lo];
+            const int j = A.list[(size_t)k * A.list_stride + (b0 + lo)];
+            double Rx = 0.0, Ry = 0.0, Rz = 0.0;
+            const int acts = contact_eval(N, A.pairs, s_pos[lo], A.pos_in[j], Rx, Ry, Rz);
+            double* r = s_R + 3 * (w - base);
+            r[0] = Rx;
+            r[1] = Ry;
+            r[2] = Rz;
+            s_Rf[w - base] = (unsigned char)acts;
+        }
+        __syncthreads();
+        if (active) {
+            const int e0 = max(off, base), e1 = min(off + nc, lim);
+            for (int w = e0; w < e1; ++w) {
+                if (s_Rf[w - base]) {
+                    const double* r = s_R + 3 * (w - base);
+                    Fx += r[0];
+                    Fy += r[1];
+                    Fz += r[2];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!active) return;
+    if (FORCES_ONLY) {
+        A.force[i] = make_float4((float)Fx, (float)Fy, (float)Fz, 0.0f);
+        return;
+    }
+    /* statuses after this step (kernel.cl:396-397, 278-284) */
+    const unsigned st0 = s_stat[tid + 2];
+    unsigned st = st0;
+    if ((s_tsp[tid + 2] & 2)) st &= ~1u;
+    if ((st0 & 2) && (s_flag[tid + 2] & FN_CH_ANGLE) && !s_tan[tid + 1]) st &= ~2u;
+    if (st != st0) A.ch_status[i] = (unsigned char)st;
+    kick_drift_store<DAMP, DRIFT, STORE_V>(A, N, i, p, Fx, Fy, Fz);
+}
+
 template <bool STORE_V>
 __global__ void __launch_bounds__(512) k_drift(const StepArgs A) {
     const FnTile t = A.tiles[blockIdx.x];
@@ -647,6 +934,27 @@ __device__ __forceinline__ bool list_candidate(const FnNet& N, const FnPair* __r
     return false;
 }
 
+/* The rest of BuildContactList's test (kernel.cl:574-586, 630-659) once the
+   (minimum-image) squared distance is known: exclusion of bonded
+   neighbours, then the listing radius of the pair kind.  Same answer as
+   list_candidate. */
+__device__ __forceinline__ bool list_accept(const FnNet& N, const FnPair* __restrict__ pairs,
+                                            double length, double4 pi, int4 bi, double4 pj,
+                                            int4 bj) {
+    if (bi.x == bj.x && abs(bi.y - bj.y) <= 1) return false;
+    const int kind = pairs[N.pair_base + getadress(bi.z, bj.z, N.types_num)].kind;
+    if (kind == 1 || kind == 3) return length < N.cutoff_sq;
+    if (kind == 2) {
+        const double si = (double)__int_as_float(bi.w), sj = (double)__int_as_float(bj.w);
+        const double ri = (double)w_radius(pi.w), rj = (double)w_radius(pj.w);
+        const double min_skin = (si > sj) ? sj : si;
+        const double max_radius = (ri > rj) ? ri : rj;
+        const double lim = max_radius + min_skin;
+        return length < lim * lim;
+    }
+    return false;
+}
+
 /* Network owning bead i (networks hold consecutive bead ranges). */
 __device__ __forceinline__ int net_of_bead(const FnNet* __restrict__ nets, int n_nets, int i) {
     int lo = 0, hi = n_nets - 1;
@@ -672,7 +980,7 @@ __device__ __forceinline__ void scan_run(const RebuildArgs& R, const FnNet& N, i
         double length = rx * rx + ry * ry + rz * rz;
         if (N.list_mi) length = min_image(N, rx, ry, rz, length, N.list_mi);
         if (!(length < N.list_r2_max)) continue; /* listed by no pair kind */
-        if (list_candidate(N, R.pairs, pi, bi, pj, R.binfo[j])) {
+        if (list_accept(N, R.pairs, length, pi, bi, pj, R.binfo[j])) {
             if (n < R.list_cap) out[(size_t)n * R.list_stride] = j;
             ++n;
         }
@@ -844,12 +1152,21 @@ __global__ void k_observe_partial(const ObserveArgs O) {
             z += (double)f.z;
         }
     }
-    for (int s = O.spring_begin + blockIdx.x * blockDim.x + tid; s < O.spring_end;
-         s += gridDim.x * blockDim.x)
-        nb += O.sp_status[s] == 0;
-    for (int a = O.angle_begin + blockIdx.x * blockDim.x + tid; a < O.angle_end;
-         a += gridDim.x * blockDim.x)
-        na += O.an_status[a] == 0;
+    if (O.ch_flags) {
+        for (int i = O.bead_begin + blockIdx.x * blockDim.x + tid; i < O.bead_end;
+             i += gridDim.x * blockDim.x) {
+            const unsigned f = O.ch_flags[i], st = O.ch_status[i];
+            nb += (f & FN_CH_SPRING) && !(st & 1);
+            na += (f & FN_CH_ANGLE) && !(st & 2);
+        }
+    } else {
+        for (int s = O.spring_begin + blockIdx.x * blockDim.x + tid; s < O.spring_end;
+             s += gridDim.x * blockDim.x)
+            nb += O.sp_status[s] == 0;
+        for (int a = O.angle_begin + blockIdx.x * blockDim.x + tid; a < O.angle_end;
+             a += gridDim.x * blockDim.x)
+            na += O.an_status[a] == 0;
+    }
     sx[tid] = x;
     sy[tid] = y;
     sz[tid] = z;
@@ -942,6 +1259,50 @@ cudaError_t launch_step_tiled(const StepArgs& A, int ntiles, int block, bool dam
             k_step_tiled<false, false, false><<<ntiles, block, sm, s>>>(A);
         }
     }
+    return cudaGetLastError();
+}
+
+template <bool DAMP, bool DRIFT, bool STORE_V, bool FO>
+static cudaError_t set_chain_smem(size_t bytes) {
+    return cudaFuncSetAttribute(k_step_chain<DAMP, DRIFT, STORE_V, FO>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t prepare_step_chain(size_t bytes) {
+    cudaError_t e;
+    if ((e = set_chain_smem<true, true, true, false>(bytes))) return e;
+    if ((e = set_chain_smem<true, false, false, false>(bytes))) return e;
+    if ((e = set_chain_smem<false, true, true, false>(bytes))) return e;
+    if ((e = set_chain_smem<false, true, false, false>(bytes))) return e;
+    if ((e = set_chain_smem<false, false, false, false>(bytes))) return e;
+    return set_chain_smem<false, false, false, true>(bytes);
+}
+
+cudaError_t launch_step_chain(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
+                              bool store_v, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    const size_t sm = step_chain_smem(block);
+    if (damp) {
+        if (do_drift)
+            k_step_chain<true, true, true, false><<<ntiles, block, sm, s>>>(A, 0);
+        else
+            k_step_chain<true, false, false, false><<<ntiles, block, sm, s>>>(A, 0);
+    } else {
+        if (do_drift) {
+            if (store_v)
+                k_step_chain<false, true, true, false><<<ntiles, block, sm, s>>>(A, 0);
+            else
+                k_step_chain<false, true, false, false><<<ntiles, block, sm, s>>>(A, 0);
+        } else {
+            k_step_chain<false, false, false, false><<<ntiles, block, sm, s>>>(A, 0);
+        }
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forces_chain(const StepArgs& A, int ntiles, int block, int terms, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    k_step_chain<false, false, false, true><<<ntiles, block, step_chain_smem(block), s>>>(A, terms);
     return cudaGetLastError();
 }
 

@@ -54,6 +54,13 @@ struct StepArgs {
     const int* an_slot;        /* per bead entry: tile angle slot << 2 | role */
     int max_tile_sp;
     int max_tile_an;
+    /* chain form (every spring joins beads j, j+1; every angle is centred on
+       its middle bead): per-bead records instead of incidence lists */
+    const float4* ch_sp;          /* spring (j, j+1): rest, k, c1, c2 */
+    const float2* ch_an;          /* angle centred on j: theta0, k */
+    const unsigned char* ch_flags; /* FN_CH_* bits */
+    unsigned char* ch_status;     /* bit 0 spring (j, j+1) alive, bit 1 angle alive */
+    int nb;
 };
 
 /* dynamic shared memory of the tiled step kernel */
@@ -61,6 +68,61 @@ inline size_t step_tiled_smem(int max_sp, int max_an) {
     return sizeof(double) * 3 * (size_t)max_sp + sizeof(double) * 6 * (size_t)max_an +
            (size_t)max_sp + (size_t)max_an + 16;
 }
+
+/* chain flag bits */
+enum {
+    FN_CH_SPRING = 1,      /* bead has a spring to bead j+1 */
+    FN_CH_SP_REV = 2,      /* that spring lists j+1 as p1 */
+    FN_CH_SP_FL = 4,       /* HR_FL (else HR) */
+    FN_CH_SP_INERT = 8,    /* spring type outside HR/HR_FL: never acts */
+    FN_CH_ANGLE = 16,      /* bead is the centre of an angle */
+    FN_CH_AN_REV = 32,     /* that angle lists j+1 as b1 */
+    FN_CH_AN_FL = 64       /* HR_FL angle (dies with its springs) */
+};
+
+/* Byte offsets of the chain step kernel's dynamic shared memory for blocks
+   of `block` threads (one layout for host sizing and device carving). */
+struct ChainSmem {
+    size_t img, spf, ang, flag, stat, tsp, tan, pos, off, ws, res, resf, total;
+};
+
+__host__ __device__ inline size_t smem_align(size_t o, size_t a) { return (o + a - 1) / a * a; }
+
+__host__ __device__ inline ChainSmem chain_smem_layout(int block) {
+    ChainSmem L;
+    const size_t h = (size_t)block + 4;
+    size_t o = 0;
+    L.img = o;  /* image positions of beads b0-2 .. b0+n+1, 3 doubles each */
+    o += 24 * h;
+    L.spf = o;  /* spring forces, lower bead b0-2 .. b0+n */
+    o += 24 * h;
+    L.ang = o;  /* angle pa, pc, centre b0-1 .. b0+n */
+    o += 48 * h;
+    L.flag = o; /* bead flags */
+    o += h;
+    L.stat = o; /* bead statuses */
+    o += h;
+    L.tsp = o;  /* spring term flags */
+    o += h;
+    L.tan = o;  /* angle term flags */
+    o += h;
+    o = smem_align(o, 32);
+    L.pos = o;  /* own wrapped positions, double4 */
+    o += 32 * (size_t)block;
+    L.off = o;  /* contact offsets, block + 1 ints */
+    o += 4 * ((size_t)block + 1);
+    L.ws = o;   /* scan scratch, 34 ints */
+    o += 4 * 34;
+    o = smem_align(o, 16);
+    L.res = o;  /* contact results of one chunk (2 * block items, 3 doubles) */
+    o += 48 * (size_t)block;
+    L.resf = o; /* contact result flags */
+    o += 2 * (size_t)block;
+    L.total = smem_align(o, 16);
+    return L;
+}
+
+inline size_t step_chain_smem(int block) { return chain_smem_layout(block).total; }
 
 struct RebuildArgs {
     const FnTile* tiles;
@@ -83,6 +145,8 @@ struct RebuildArgs {
 };
 
 struct ObserveArgs {
+    const unsigned char* ch_flags; /* chain form: statuses per bead */
+    const unsigned char* ch_status;
     const double4* pos;
     const float4* force;
     const signed char* sp_status;
@@ -99,6 +163,10 @@ cudaError_t launch_step(const StepArgs& A, int ntiles, int block, bool damp, boo
 cudaError_t launch_step_tiled(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
                               bool store_v, cudaStream_t s);
 cudaError_t prepare_step_tiled(size_t smem_bytes);
+cudaError_t launch_step_chain(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
+                              bool store_v, cudaStream_t s);
+cudaError_t launch_forces_chain(const StepArgs& A, int ntiles, int block, int terms, cudaStream_t s);
+cudaError_t prepare_step_chain(size_t smem_bytes);
 cudaError_t launch_drift(const StepArgs& A, int ntiles, int block, bool store_v, cudaStream_t s);
 cudaError_t launch_forces_only(const StepArgs& A, int ntiles, int block, int terms, cudaStream_t s);
 cudaError_t launch_reset_energy(float4* force, float4* vel, float4* vold, int n, cudaStream_t s);

@@ -46,13 +46,14 @@ class FnNetworkDesc(C.Structure):
 
 class FnConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("cell_capacity", C.c_int), ("list_capacity", C.c_int),
-                ("reorder", C.c_int), ("use_graphs", C.c_int), ("block_size", C.c_int)]
+                ("reorder", C.c_int), ("use_graphs", C.c_int), ("block_size", C.c_int),
+                ("chain_mode", C.c_int)]
 
 
 class FnStats(C.Structure):
     _fields_ = [("cell_overflow", C.c_longlong), ("list_overflow", C.c_longlong),
                 ("rebuilds", C.c_longlong), ("steps", C.c_longlong), ("block_size", C.c_int),
-                ("n_networks", C.c_int), ("n_beads", C.c_longlong),
+                ("bond_path", C.c_int), ("n_networks", C.c_int), ("n_beads", C.c_longlong),
                 ("device_bytes", C.c_longlong)]
 
 
@@ -162,11 +163,12 @@ class Simulation:
     """One device context holding one network or a batched ensemble."""
 
     def __init__(self, models, device: int = 0, cell_capacity: int = 64, list_capacity: int = 64,
-                 reorder: bool = True, use_graphs: bool = False, block_size: int = 0):
+                 reorder: bool = True, use_graphs: bool = False, block_size: int = 0,
+                 chain: bool = True):
         self.lib = load()
         self.models = [models] if isinstance(models, Model) else list(models)
         cfg = FnConfig(device, cell_capacity, list_capacity, int(reorder), int(use_graphs),
-                       block_size)
+                       block_size, 0 if chain else 2)
         h = C.c_void_p()
         rc = self.lib.fn_create(C.byref(cfg), C.byref(h))
         if rc != FN_OK:

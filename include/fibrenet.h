@@ -111,7 +111,9 @@ typedef struct fn_config {
     int list_capacity;  /* contacts kept per bead (full list) */
     int reorder;        /* 1: renumber beads in Morton order of their fibre */
     int use_graphs;     /* 1: replay steps as CUDA graphs */
-    int block_size;     /* threads per block for the step kernel; 0 = tune */
+    int block_size;     /* threads per block for the step kernel; 0 = default */
+    int chain_mode;     /* 0 auto: per-bead bond records when the model is in
+                           chain form (fibres); 2 never (incidence lists) */
 } fn_config;
 
 /* Counters read back from the device. */
@@ -121,6 +123,7 @@ typedef struct fn_stats {
     long long rebuilds;        /* contact-list rebuilds done */
     long long steps;           /* time steps done */
     int block_size;            /* step-kernel block size in use */
+    int bond_path;             /* 0 per-bead incidence, 1 per-tile incidence, 2 chain records */
     int n_networks;
     long long n_beads;
     long long device_bytes;    /* device memory held by the context */

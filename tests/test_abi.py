@@ -42,7 +42,7 @@ def test_no_device_means_error_not_fallback():
         pytest.skip("a GPU is present")
     from fibrenet_b200 import native
     lib = native.load()
-    cfg = native.FnConfig(0, 64, 64, 1, 0, 0)
+    cfg = native.FnConfig(0, 64, 64, 1, 0, 0, 0)
     h = C.c_void_p()
     rc = lib.fn_create(C.byref(cfg), C.byref(h))
     assert rc == 2  # FN_ERR_CUDA

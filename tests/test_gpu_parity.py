@@ -27,6 +27,7 @@ FORCE_TOL = 1e-5  # relative, norm-wise, FP32 result vs FP64 reference (north-st
 def sim(model, **kw):
     from fibrenet_b200.native import Simulation
     kw.setdefault("reorder", False)
+    kw.setdefault("chain", True)
     kw.setdefault("list_capacity", 256)
     return Simulation(model, **kw)
 
@@ -200,3 +201,77 @@ def test_bad_model_is_rejected():
     m.s_p2[0] = 10_000
     with pytest.raises(NativeError):
         sim(m)
+
+
+def _crosslinked(seed=6):
+    """Fibres plus random cross-links between nearby beads of different
+    fibres: not chain form, so the incidence path runs."""
+    m = g.plain_network(seed=seed, fibres=30, beads=20, box=(20.0, 20.0, 6.0), z_range=(1.0, 5.0))
+    img = m.img
+    d2 = ((img[:, None, :] - img[None, :, :]) ** 2).sum(-1)
+    close = np.argwhere((d2 < 2.25) & (m.tag[:, None] < m.tag[None, :]))
+    extra = [tuple(x) for x in close[::3][:60]]
+    assert len(extra) > 10
+    e = np.array(extra, np.int32)
+    n = len(e)
+    m.s_type = np.concatenate([m.s_type, np.full(n, 1, np.int32)])
+    m.s_tag = np.concatenate([m.s_tag, np.full(n, -1, np.int32)])
+    m.s_p1 = np.concatenate([m.s_p1, e[:, 0]])
+    m.s_p2 = np.concatenate([m.s_p2, e[:, 1]])
+    d = np.linalg.norm(img[e[:, 0]] - img[e[:, 1]], axis=1)
+    m.s_rest = np.concatenate([m.s_rest, d.astype(np.float32).astype(np.float64)])
+    m.s_k = np.concatenate([m.s_k, np.full(n, 80.0)])
+    m.s_c1 = np.concatenate([m.s_c1, np.full(n, 1000.0)])
+    m.s_c2 = np.concatenate([m.s_c2, np.full(n, 2.0)])
+    return m
+
+
+def _reversed(m):
+    """Same chains with every spring and angle listed the other way round."""
+    m = m.normalised().copy()
+    m.s_p1, m.s_p2 = m.s_p2.copy(), m.s_p1.copy()
+    m.a_b1, m.a_b3 = m.a_b3.copy(), m.a_b1.copy()
+    m.a_s1, m.a_s2 = m.a_s2.copy(), m.a_s1.copy()
+    return m
+
+
+@pytest.mark.parametrize("kind", ["chain", "reversed", "crosslinked"])
+def test_bond_paths_bit_exact_vs_mirror(oracle_built, kind):
+    if kind == "crosslinked":
+        m = _crosslinked()
+    else:
+        m = g.tensile_network(seed=8, fibres=40, beads=20, box=(40.0, 30.0, 8.0), z_range=(1.0, 7.0),
+                              fail_mu=np.log(0.5), fail_sigma=0.4, clamp_lo=2.0, clamp_hi=38.0,
+                              pull=0.5, cell=2.5)
+        m.a_type[:] = 1  # HR_FL angles: die with their springs
+        if kind == "reversed":
+            m = _reversed(m)
+    o = po.OracleSim(m, po.MODE_MIRROR, cell_cap=64, list_cap=64)
+    o.run(150)
+    for chain in (True, False):
+        s = sim(m, list_capacity=64, chain=chain)
+        want_path = 2 if (chain and kind != "crosslinked") else 1
+        assert s.stats()["bond_path"] == want_path
+        s.step(150)
+        for f in FIELDS:
+            np.testing.assert_array_equal(s.get(f), o.get(f), err_msg=f"{kind} chain={chain} {f}")
+        np.testing.assert_array_equal(s.status()[0], o.status()[0])
+        np.testing.assert_array_equal(s.status()[1], o.status()[1])
+    assert (o.status()[0] == 0).sum() > 0
+
+
+@pytest.mark.parametrize("chain", [True, False])
+def test_forces_only_paths(oracle_built, chain):
+    m = g.plain_network(seed=22, fibres=60, beads=30).fp32_representable()
+    rng = np.random.default_rng(3)
+    m.img = (m.img + rng.normal(0.0, 0.03, m.img.shape)).astype(np.float32).astype(np.float64)
+    m.pos = np.mod(m.img, np.asarray(m.settings.box))
+    r = po.OracleSim(m, po.MODE_REF)
+    r.rebuild()
+    s = sim(m, list_capacity=64, chain=chain)
+    s.rebuild()
+    for terms in [(1, 1, 1), (1, 0, 0), (0, 1, 0), (0, 0, 1)]:
+        r.forces_only(*terms)
+        s.forces_only(*terms)
+        e = rel_norm(s.get("force"), r.get("force"))
+        assert e <= FORCE_TOL, (terms, e)
