@@ -14,6 +14,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -1432,3 +1433,81 @@ FN_API int fn_forces_only(fn_ctx* c, int terms) {
 }
 
 }  // extern "C"
+
+/* ======================================================================== */
+/* Observables without any device allocation.                               */
+
+/* Partial sums of the observables reduction: one slot of 5 doubles per block
+   of 256 items, for at most FN_OBSERVE_NOALLOC_MAX_BLOCKS blocks.  It lives in
+   the library image, so every GPU that loads the library holds these 320 KB
+   until the process exits, and every call shares them. */
+#define FN_OBSERVE_NOALLOC_MAX_BLOCKS 8192
+static __device__ __align__(256) double fn_observe_scratch[5 * FN_OBSERVE_NOALLOC_MAX_BLOCKS];
+
+namespace {
+
+/* Device address of fn_observe_scratch on each device, looked up once per
+   device.  In host code the array's name only stands in for the symbol; its
+   address on a device comes from cudaGetSymbolAddress with that device
+   current. */
+constexpr int FN_NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_scratch[FN_NOALLOC_MAX_DEVICES] = {};
+
+int noalloc_scratch(fn_ctx* c, double** out) {
+    const int dev = c->cfg.device;
+    if (dev < 0 || dev >= FN_NOALLOC_MAX_DEVICES)
+        return fail(c, FN_ERR_UNSUPPORTED, "fn_observe_noalloc: device ordinal beyond 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_scratch[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, fn_observe_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(c, FN_ERR_CUDA, std::string("fn_observe_noalloc: cudaGetSymbolAddress: ") +
+                                            cudaGetErrorString(e));
+        g_noalloc_scratch[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_scratch[dev];
+    return FN_OK;
+}
+
+}  // namespace
+
+extern "C" FN_API int fn_observe_noalloc(fn_ctx* c, int net, int reaction_type, double* out_device) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!out_device || net < 0 || net >= c->n_nets)
+        return fail(c, FN_ERR_ARG, "fn_observe_noalloc: bad arguments");
+    const NetHost& h = c->info[net];
+    const long long span = std::max({(long long)(h.bead_end - h.bead_begin),
+                                     (long long)(h.spring_end - h.spring_begin),
+                                     (long long)(h.angle_end - h.angle_begin), 1LL});
+    const long long nblocks = (span + 255) / 256;
+    if (nblocks > FN_OBSERVE_NOALLOC_MAX_BLOCKS)
+        return fail(c, FN_ERR_CAPACITY,
+                    "fn_observe_noalloc: network " + std::to_string(net) + " has " +
+                        std::to_string(span) + " beads/springs/angles; the static scratch holds " +
+                        std::to_string((long long)FN_OBSERVE_NOALLOC_MAX_BLOCKS * 256) +
+                        " at most (use fn_observe)");
+    CK(cudaSetDevice(c->cfg.device));
+    double* scratch = nullptr;
+    r = noalloc_scratch(c, &scratch);
+    if (r) return r;
+    fn::ObserveArgs O{};
+    O.ch_flags = c->chain ? c->ch_flags.p : nullptr;
+    O.ch_status = c->chain ? c->ch_status.p : nullptr;
+    O.pos = c->pos[c->cur].p;
+    O.force = c->force.p;
+    O.sp_status = c->sp_status.p;
+    O.an_status = c->an_status.p;
+    O.bead_begin = h.bead_begin;
+    O.bead_end = h.bead_end;
+    O.spring_begin = h.spring_begin;
+    O.spring_end = h.spring_end;
+    O.angle_begin = h.angle_begin;
+    O.angle_end = h.angle_end;
+    O.reaction_type = reaction_type;
+    O.partial = scratch;
+    CK(fn::launch_observe(O, (int)nblocks, out_device, c->stream));
+    return FN_OK;
+}

@@ -82,6 +82,7 @@ SIGNATURES = {
     "fn_set_status": (C.c_int, [C.c_void_p, _I, _I]),
     "fn_observe": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(FnObservables)]),
     "fn_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FnStats)]),
+    "fn_observe_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "fn_get_cells": (C.c_int, [C.c_void_p, _I, _I, C.c_longlong]),
     "fn_get_lists": (C.c_int, [C.c_void_p, _I, _I, C.c_int]),
     "fn_n_cells": (C.c_longlong, [C.c_void_p]),
@@ -268,6 +269,13 @@ class Simulation:
         self._check(self.lib.fn_observe(self.h, net, reaction_type, C.byref(o)))
         return {"reaction": np.array(o.reaction[:]), "broken": int(o.broken),
                 "angles_dead": int(o.angles_dead)}
+
+    def observe_noalloc(self, out_device_ptr: int, net: int = 0, reaction_type: int = -1) -> None:
+        """fn_observe without device allocation: writes 5 doubles (reaction
+        x, y, z, broken springs, dead angles) to a caller-owned device buffer
+        asynchronously; call sync() before reading it."""
+        self._check(self.lib.fn_observe_noalloc(self.h, net, reaction_type,
+                                                C.c_void_p(out_device_ptr)))
 
     def stats(self) -> dict:
         s = FnStats()

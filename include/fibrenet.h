@@ -206,6 +206,21 @@ FN_API int fn_observe(fn_ctx* ctx, int net, int reaction_type, fn_observables* o
 
 FN_API int fn_get_stats(fn_ctx* ctx, fn_stats* out);
 
+/* The observables of fn_observe for callers that cannot allocate device
+   memory when they need them, e.g. code that runs while a CUDA graph is being
+   captured or inside a loop where a cudaMalloc (which may synchronise the
+   device) is not allowed.  No counterpart in the reference.  Writes
+   {reaction x, y, z, broken springs, dead angles} as 5 doubles to the
+   caller's device buffer out_device, asynchronously on the context's stream
+   (read it after fn_sync).  Calls no cudaMalloc/cudaFree: its scratch is a
+   fixed 320 KB array in the library, which every GPU that loads the library
+   keeps until exit.  Networks with more than 2,097,152 beads, springs or
+   angles are rejected with FN_ERR_CAPACITY (use fn_observe).  The first call
+   on a device looks up the scratch's device address; make it before any
+   stream capture.  All calls share the scratch: calls that overlap on the GPU
+   (other streams or contexts on the same device) race. */
+FN_API int fn_observe_noalloc(fn_ctx* ctx, int net, int reaction_type, double* out_device);
+
 /* Grid and contact-list inspection (tests): cell of each bead (-1 outside
    the grid or beyond the cell capacity), the raw count of each cell, and
    each bead's contacts (raw count and up to cap partner ids), all in upload
