@@ -15,8 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfibrenet.so")
-SOURCES = ["fn_kernels.cu", "fn_engine.cu", "fn_generate.cpp"]
-HEADERS = ["fn_kernels.h", "fn_types.h", "fn_detmath.h"]
+CLI = os.path.join(HERE, "fibrenet_run")
+SOURCES = ["fn_kernels.cu", "fn_engine.cu", "fn_generate.cpp", "fn_io.cpp"]
+HEADERS = ["fn_kernels.h", "fn_types.h", "fn_detmath.h", "fn_cli.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -34,11 +35,11 @@ def nvcc() -> str:
 
 
 def _stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps += [os.path.join(ROOT, "include", h) for h in ("fibrenet.h", "fibrenet_generate.h")]
+    deps += [os.path.join(ROOT, "include", h) for h in ("fibrenet.h", "fibrenet_generate.h", "fibrenet_io.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
@@ -53,6 +54,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if out.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + out.stdout + out.stderr)
     os.replace(LIB + ".tmp", LIB)
+    cli = [nvcc(), "-O2", "-std=c++17", "-o", CLI, os.path.join(CSRC, "fn_cli.cpp"), "-L", HERE,
+           "-lfibrenet", "-Xlinker", "-rpath,$ORIGIN"]
+    out = subprocess.run(cli, capture_output=True, text=True, cwd=CSRC)
+    if out.returncode != 0:
+        raise RuntimeError("building the command-line runner failed:\n" + out.stdout + out.stderr)
     return LIB
 
 
