@@ -700,56 +700,56 @@ __global__ void __launch_bounds__(512) k_step_chain(const StepArgs A, int terms)
         }
     }
 
-    /* contacts, load-balanced over the block: item w of the block's
-       concatenated lists is evaluated by thread w mod blockDim, the results
-       land in shared memory, and each bead adds its own items in list order
-       (the order of the sequential loop, so the sums are identical) */
-    double4* s_pos = reinterpret_cast<double4*>(smem_raw + L.pos);
-    int* s_off = reinterpret_cast<int*>(smem_raw + L.off);
-    int* s_ws = reinterpret_cast<int*>(smem_raw + L.ws);
-    double* s_R = reinterpret_cast<double*>(smem_raw + L.res);
-    unsigned char* s_Rf = smem_raw + L.resf;
-    const int chunk = 2 * blockDim.x;
-    if (active) s_pos[tid] = p;
-    int total;
-    const int off = block_scan_any(nc, s_ws, total);
-    s_off[tid] = off;
-    if (tid == 0) s_off[blockDim.x] = total;
-    __syncthreads();
-    for (int base = 0; base < total; base += chunk) {
-        const int lim = min(base + chunk, total);
-        for (int w = base + tid; w < lim; w += blockDim.x) {
-            int lo = 0, hi = n - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_off[mid] <= w)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            const int k = w - s_off[lo];
-            const int j = A.list[(size_t)k * A.list_stride + (b0 + lo)];
-            double Rx = 0.0, Ry = 0.0, Rz = 0.0;
-            const int acts = contact_eval(N, A.pairs, s_pos[lo], A.pos_in[j], Rx, Ry, Rz);
-            double* r = s_R + 3 * (w - base);
-            r[0] = Rx;
-            r[1] = Ry;
-            r[2] = Rz;
-            s_Rf[w - base] = (unsigned char)acts;
+    /* contacts, load-balanced inside each warp: the warp's beads' list items
+       are taken 32 at a time, lane l evaluating item (window base + l); a
+       32-byte map tells each lane whose item it holds, results go to shared
+       memory and every bead then adds its own items in list order (the order
+       of a sequential loop over its list, so the sums are identical).  Only
+       warp barriers are involved. */
+    {
+        const int lane = tid & 31, wid = tid >> 5;
+        unsigned char* s_map = smem_raw + L.wmap + 32 * (size_t)wid;
+        double* s_R = reinterpret_cast<double*>(smem_raw + L.wres) + 3 * 32 * (size_t)wid;
+        unsigned char* s_Rf = smem_raw + L.wresf + 32 * (size_t)wid;
+        const double4* s_pos = reinterpret_cast<const double4*>(smem_raw + L.pos);
+        double4* s_pos_w = reinterpret_cast<double4*>(smem_raw + L.pos);
+        if (active) s_pos_w[tid] = p;
+        int off = nc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= o) off += y;
         }
-        __syncthreads();
-        if (active) {
-            const int e0 = max(off, base), e1 = min(off + nc, lim);
-            for (int w = e0; w < e1; ++w) {
-                if (s_Rf[w - base]) {
-                    const double* r = s_R + 3 * (w - base);
-                    Fx += r[0];
-                    Fy += r[1];
-                    Fz += r[2];
+        const int total = __shfl_sync(0xffffffffu, off, 31);
+        off -= nc; /* exclusive */
+        __syncwarp();
+        for (int base = 0; base < total; base += 32) {
+            const int lim = min(base + 32, total);
+            for (int w = max(off, base); w < min(off + nc, lim); ++w) s_map[w - base] = (unsigned char)lane;
+            __syncwarp();
+            const int w = base + lane;
+            const int b = w < lim ? s_map[lane] : 0;
+            const int ob = __shfl_sync(0xffffffffu, off, b);
+            if (w < lim) {
+                const int ib = (tid & ~31) + b; /* block-local bead of the item */
+                const int j = A.list[(size_t)(w - ob) * A.list_stride + (b0 + ib)];
+                double Rx = 0.0, Ry = 0.0, Rz = 0.0;
+                const int acts = contact_eval(N, A.pairs, s_pos[ib], A.pos_in[j], Rx, Ry, Rz);
+                s_R[3 * lane] = Rx;
+                s_R[3 * lane + 1] = Ry;
+                s_R[3 * lane + 2] = Rz;
+                s_Rf[lane] = (unsigned char)acts;
+            }
+            __syncwarp();
+            for (int q = max(off, base); q < min(off + nc, lim); ++q) {
+                if (s_Rf[q - base]) {
+                    Fx += s_R[3 * (q - base)];
+                    Fy += s_R[3 * (q - base) + 1];
+                    Fz += s_R[3 * (q - base) + 2];
                 }
             }
+            __syncwarp();
         }
-        __syncthreads();
     }
     if (!active) return;
     if (FORCES_ONLY) {

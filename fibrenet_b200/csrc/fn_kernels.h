@@ -83,7 +83,7 @@ enum {
 /* Byte offsets of the chain step kernel's dynamic shared memory for blocks
    of `block` threads (one layout for host sizing and device carving). */
 struct ChainSmem {
-    size_t img, spf, ang, flag, stat, tsp, tan, pos, off, ws, res, resf, total;
+    size_t img, spf, ang, flag, stat, tsp, tan, pos, wres, wmap, wresf, total;
 };
 
 __host__ __device__ inline size_t smem_align(size_t o, size_t a) { return (o + a - 1) / a * a; }
@@ -109,15 +109,12 @@ __host__ __device__ inline ChainSmem chain_smem_layout(int block) {
     o = smem_align(o, 32);
     L.pos = o;  /* own wrapped positions, double4 */
     o += 32 * (size_t)block;
-    L.off = o;  /* contact offsets, block + 1 ints */
-    o += 4 * ((size_t)block + 1);
-    L.ws = o;   /* scan scratch, 34 ints */
-    o += 4 * 34;
-    o = smem_align(o, 16);
-    L.res = o;  /* contact results of one chunk (2 * block items, 3 doubles) */
-    o += 48 * (size_t)block;
-    L.resf = o; /* contact result flags */
-    o += 2 * (size_t)block;
+    L.wres = o; /* per warp: contact results of one window of 32 items */
+    o += 24 * (size_t)block;
+    L.wmap = o; /* per warp: item -> lane map of the window */
+    o += (size_t)block;
+    L.wresf = o; /* per warp: result flags */
+    o += (size_t)block;
     L.total = smem_align(o, 16);
     return L;
 }
