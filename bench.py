@@ -46,6 +46,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
+    p.add_argument("--workload", choices=["tensile", "ensemble"], default="tensile",
+                   help="tensile: the 1M-bead network (default, the headline); ensemble: 256 "
+                        "independent networks batched in one context vs run one by one")
+    p.add_argument("--networks", type=int, default=256)
     return p.parse_args()
 
 
@@ -377,10 +381,71 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_ensemble(args):
+    """Batched ensemble: the networks in one context (one launch per kernel
+    for all of them, steps replayed as CUDA graphs, tuned block size) against
+    the same networks each in its own context, run one after the other."""
+    import torch
+
+    from fibrenet_b200 import generate as g
+    from fibrenet_b200.native import Simulation
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    ms = g.ensemble_networks(seed=3, n_networks=args.networks)
+    nb = sum(m.n_beads for m in ms)
+    K = args.steps
+
+    def timed(sim, steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sim.sync()
+        torch.cuda.synchronize()
+        e0.record()
+        sim.step(steps)
+        sim.sync()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    batched = Simulation(ms, list_capacity=32, reorder=True, use_graphs=True)
+    batched.step(max(args.warmup, 3))
+    block = batched.autotune(16)
+    batched.step(8)
+    clocks = ClockSampler(0)
+    clocks.start()
+    t_batched = timed(batched, K)
+    clk = clocks.stop()
+    batched.enable_timing(True)
+    batched.step(16)
+    kt = batched.kernel_time()
+    batched.close()
+    t_single = 0.0
+    for m in ms:
+        one = Simulation(m, list_capacity=32, reorder=True, use_graphs=True)
+        one.step(max(args.warmup, 3))
+        t_single += timed(one, K)
+        one.close()
+    v_b = nb * K / (t_batched / 1e3)
+    v_s = nb * K / (t_single / 1e3)
+    line = {"metric": "bead-steps/s (256-network ensemble, batched in one launch per kernel)",
+            "value": v_b, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": max(args.warmup, 3),
+            "ms_per_step": t_batched / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": f"ensemble_{len(ms)}", "networks": len(ms), "beads": nb,
+                       "fibres_per_network": "U[50, 2000] x 50 beads", "block_size": block,
+                       "graphs": True},
+            "one_by_one": {"value": v_s, "ms_per_step_all_networks": t_single / K},
+            "batched_over_one_by_one": v_b / v_s,
+            "step_kernel_ms": kt["step_ms"], "rebuild_ms": kt["rebuild_ms"], "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
     else:
         run_ours(args)
 

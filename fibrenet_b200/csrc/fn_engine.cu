@@ -14,7 +14,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -128,6 +130,10 @@ struct fn_ctx {
     long long device_bytes = 0;
     long long steps_done = 0, rebuilds_done = 0;
 
+    /* captured step segments: (parity, length, ends the call) -> graph */
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+    long long graph_launches = 0;
+
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_step, ev_rebuild;
@@ -182,7 +188,13 @@ cudaError_t h2d(fn_ctx* c, DevBuf<T>& b, const std::vector<T>& v) {
     return cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c->stream);
 }
 
+void drop_graphs(fn_ctx* c) {
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+}
+
 void free_all(fn_ctx* c) {
+    drop_graphs(c);
     for (int k = 0; k < 2; ++k) {
         dfree(c, c->pos[k]);
         dfree(c, c->img[k]);
@@ -541,6 +553,7 @@ bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<
 }
 
 int set_block(fn_ctx* c, int block) {
+    drop_graphs(c);
     std::vector<FnTile> t;
     int n = build_tiles(c, block, t);
     CK(cudaStreamSynchronize(c->stream));
@@ -674,6 +687,55 @@ int launch_one_step(fn_ctx* c, bool do_drift, bool store_v) {
     return FN_OK;
 }
 
+/* One segment of a RunSimulationLoop call: the contact rebuild that opens
+   every grid_update_freq steps, then `len` steps; when `tail` the segment
+   ends the call, so its last step does not drift and the step before it
+   keeps the predicted velocity. */
+int launch_segment(fn_ctx* c, int len, bool tail) {
+    int r = do_rebuild(c);
+    if (r) return r;
+    for (int k = 0; k < len; ++k) {
+        const bool last = tail && k == len - 1;
+        r = launch_one_step(c, !last, tail && k == len - 2);
+        if (r) return r;
+    }
+    return FN_OK;
+}
+
+/* The segment through a CUDA graph captured on first use (kernel arguments
+   depend on the ping-pong parity, the length and whether it ends the call). */
+int run_segment(fn_ctx* c, int len, bool tail) {
+    if (!c->cfg.use_graphs || c->timing) return launch_segment(c, len, tail);
+    const auto key = std::make_tuple(c->cur, len, tail ? 1 : 0);
+    auto it = c->graphs.find(key);
+    if (it == c->graphs.end()) {
+        const int cur0 = c->cur;
+        const long long rb0 = c->rebuilds_done;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int r = launch_segment(c, len, tail);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) return fail(c, FN_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        cudaGraphExec_t x = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return fail(c, FN_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        it = c->graphs.emplace(key, x).first;
+        c->cur = cur0; /* capture recorded the launches without running them */
+        c->rebuilds_done = rb0;
+    }
+    CK(cudaGraphLaunch(it->second, c->stream));
+    c->graph_launches++;
+    c->rebuilds_done++;
+    const int drifts = tail ? len - 1 : len;
+    if (drifts & 1) c->cur = 1 - c->cur;
+    return FN_OK;
+}
+
 int check_ready(fn_ctx* c) {
     if (!c) return FN_ERR_ARG;
     if (!c->uploaded) return fail(c, FN_ERR_STATE, "no model uploaded");
@@ -732,6 +794,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     if (!c || n_networks <= 0 || !nets) return fail(c, FN_ERR_ARG, "fn_upload: bad arguments");
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
     c->uploaded = false;
     c->n_nets = n_networks;
     c->nets_h.assign(n_networks, FnNet{});
@@ -1019,17 +1082,14 @@ FN_API int fn_step(fn_ctx* c, int nsteps) {
         fn::StepArgs A = step_args(c, false);
         CK(fn::launch_drift(A, c->ntiles, c->block, c->damp || nsteps == 1, c->stream));
     }
-    int grid_update_cnt = 0; /* local, as SimulationManager.cpp:152 */
-    for (int step = 0; step < nsteps; ++step) {
-        if (grid_update_cnt == c->grid_update_freq) grid_update_cnt = 0;
-        if (grid_update_cnt == 0) {
-            r = do_rebuild(c);
-            if (r) return r;
-        }
-        const bool last = step == nsteps - 1;
-        r = launch_one_step(c, !last, step == nsteps - 2);
+    /* the rebuild counter is local to the call (SimulationManager.cpp:152),
+       so the call is a sequence of grid_update_freq-step segments, each
+       opened by a rebuild */
+    for (int done = 0; done < nsteps;) {
+        const int len = std::min(c->grid_update_freq, nsteps - done);
+        r = run_segment(c, len, done + len == nsteps);
         if (r) return r;
-        grid_update_cnt++;
+        done += len;
     }
     c->steps_done += nsteps;
     return FN_OK;
@@ -1306,6 +1366,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     std::memset(out, 0, sizeof *out);
     out->block_size = c->block;
     out->bond_path = c->chain ? 2 : (c->tiled ? 1 : 0);
+    out->graph_launches = c->graph_launches;
     out->n_networks = c->n_nets;
     out->n_beads = c->nb;
     out->device_bytes = c->device_bytes;
@@ -1414,8 +1475,81 @@ FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, doubl
     return FN_OK;
 }
 
+/* Block-size tuner: for each candidate the same `steps_per_trial` steps run
+   from one snapshot of the state (restored after every trial, so the
+   simulation does not advance), timed with CUDA events; the fastest block
+   size is kept. */
 FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
-    return fail(c, FN_ERR_UNSUPPORTED, "autotune not built yet");
+    int r = check_ready(c);
+    if (r) return r;
+    if (steps_per_trial <= 0) return fail(c, FN_ERR_ARG, "fn_autotune: steps_per_trial must be positive");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    const size_t nb = (size_t)c->nb;
+    struct Snap {
+        void* p;
+        const void* src;
+        size_t bytes;
+    };
+    std::vector<Snap> snaps;
+    auto add = [&](const void* src, size_t bytes) {
+        if (src && bytes) snaps.push_back({nullptr, src, bytes});
+    };
+    add(c->pos[c->cur].p, sizeof(double4) * nb);
+    add(c->img[c->cur].p, sizeof(double4) * nb);
+    add(c->vold.p, sizeof(float4) * nb);
+    add(c->force.p, sizeof(float4) * nb);
+    add(c->vel.p, sizeof(float4) * nb);
+    add(c->sp_status.p, (size_t)c->ns);
+    add(c->an_status.p, (size_t)c->na);
+    if (c->chain) add(c->ch_status.p, nb);
+    add(c->counters.p, sizeof(unsigned long long) * FN_CNT_N);
+    for (auto& sn : snaps) {
+        CK(cudaMalloc(&sn.p, sn.bytes));
+        CK(cudaMemcpyAsync(sn.p, sn.src, sn.bytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    const int cur0 = c->cur;
+    const long long steps0 = c->steps_done, rb0 = c->rebuilds_done;
+    const bool timing0 = c->timing;
+    c->timing = false;
+    const int candidates[] = {64, 96, 128, 192, 256, 384, 512};
+    int best = c->block;
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int b : candidates) {
+        if ((r = set_block(c, b))) break;
+        for (int rep = 0; rep < 2 && !r; ++rep) { /* first run warms up */
+            c->cur = cur0;
+            for (auto& sn : snaps)
+                CK(cudaMemcpyAsync(const_cast<void*>(sn.src), sn.p, sn.bytes, cudaMemcpyDeviceToDevice, c->stream));
+            CK(cudaEventRecord(e0, c->stream));
+            r = fn_step(c, steps_per_trial);
+            CK(cudaEventRecord(e1, c->stream));
+        }
+        if (r) break;
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = b;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->cur = cur0;
+    for (auto& sn : snaps) {
+        cudaMemcpyAsync(const_cast<void*>(sn.src), sn.p, sn.bytes, cudaMemcpyDeviceToDevice, c->stream);
+    }
+    cudaStreamSynchronize(c->stream);
+    for (auto& sn : snaps) cudaFree(sn.p);
+    c->steps_done = steps0;
+    c->rebuilds_done = rb0;
+    c->timing = timing0;
+    if (r) return r;
+    return set_block(c, best);
 }
 
 /* Forces alone at the current positions (zeroed, no base term), for the

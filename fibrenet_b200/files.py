@@ -81,32 +81,9 @@ def write_input_file(m: Model, path: str, model_path: str, output_stem: str, run
         fh.write("\n".join(L) + "\n")
 
 
-class RunInfo(C.Structure):
-    _fields_ = [("run_steps", C.c_int), ("output_freq", C.c_int), ("minimize_steps", C.c_int),
-                ("minimize_substeps", C.c_int), ("minimize_reset", C.c_int),
-                ("export_position", C.c_int), ("export_velocity", C.c_int),
-                ("export_force", C.c_int), ("has_skin_override", C.c_int), ("strict", C.c_int)]
-
-
 def _lib():
     from . import native
-    lib = native.load()
-    if not getattr(lib, "_io_ready", False):
-        lib.fn_input_read.restype = C.c_int
-        lib.fn_input_read.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
-        lib.fn_input_free.argtypes = [C.c_void_p]
-        lib.fn_input_desc.argtypes = [C.c_void_p, C.POINTER(native.FnNetworkDesc)]
-        lib.fn_input_info.argtypes = [C.c_void_p, C.POINTER(RunInfo)]
-        lib.fn_input_skin.restype = C.POINTER(C.c_double)
-        lib.fn_input_skin.argtypes = [C.c_void_p]
-        lib.fn_input_type_name.restype = C.c_char_p
-        lib.fn_input_type_name.argtypes = [C.c_void_p, C.c_int]
-        lib.fn_input_output_stem.restype = C.c_char_p
-        lib.fn_input_output_stem.argtypes = [C.c_void_p]
-        lib.fn_run_input.restype = C.c_int
-        lib.fn_run_input.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int]
-        lib._io_ready = True
-    return lib
+    return native.load()
 
 
 class InputError(ValueError):
@@ -126,7 +103,8 @@ def read_input(path: str, strict: bool = False):
         from .native import FnNetworkDesc
         d = FnNetworkDesc()
         lib.fn_input_desc(h, C.byref(d))
-        info = RunInfo()
+        from .native import FnRunInfo
+        info = FnRunInfo()
         lib.fn_input_info(h, C.byref(info))
         n, ns, na = d.n_beads, d.n_springs, d.n_angles
         nt = d.settings.n_types
@@ -160,7 +138,7 @@ def read_input(path: str, strict: bool = False):
             a_s2=arr(d.a_s2, na, i32), a_theta0=arr(d.a_theta0, na, f64), a_k=arr(d.a_k, na, f64),
         )
         skin = arr(lib.fn_input_skin(h), n, f64) if info.has_skin_override else None
-        run = {f: getattr(info, f) for f, _ in RunInfo._fields_}
+        run = {f: getattr(info, f) for f, _ in FnRunInfo._fields_}
         run["output_stem"] = lib.fn_input_output_stem(h).decode()
         return m, run, skin
     finally:

@@ -348,3 +348,26 @@ def explicit_model(settings: Settings, type_names, pairs, beads, springs=(), ang
         a_b2=acol(3, np.int32), a_b3=acol(4, np.int32), a_s1=acol(5, np.int32),
         a_s2=acol(6, np.int32), a_theta0=acol(7, np.float64), a_k=acol(8, np.float64),
     )
+
+
+def ensemble_networks(seed=3, n_networks=256, fibres_lo=50, fibres_hi=2000, beads=50, z=10.0,
+                      k_s=(50.0, 200.0), k_a=(2.0, 20.0), k_contact=50.0, dt=0.001, cell=1.0,
+                      grid_update_freq=8):
+    """Independent config-0-style networks (config 3 at its default sizes):
+    fibre counts uniform in [fibres_lo, fibres_hi], each network in its own
+    periodic box sqrt(F/200)*100 wide in x and y and z high, spring stiffness
+    uniform in k_s and angle stiffness uniform in k_a per network, penalty
+    contacts.  Returns a list of Models."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(fibres_lo, fibres_hi + 1, n_networks)
+    out = []
+    for k, F in enumerate(counts):
+        side = float(np.sqrt(F / 200.0) * 100.0)
+        ks = float(rng.uniform(*k_s))
+        ka = float(rng.uniform(*k_a))
+        m = plain_network(seed=int(rng.integers(0, 2**31 - 1)), fibres=int(F), beads=beads,
+                          box=(side, side, z), z_range=(1.0, z - 1.0), k_s=ks, k_a=ka,
+                          k_contact=k_contact, dt=dt, cell=cell, grid_update_freq=grid_update_freq)
+        m.meta.update(kind="ensemble", index=k, k_s=ks, k_a=ka)
+        out.append(m)
+    return out

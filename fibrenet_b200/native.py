@@ -54,12 +54,19 @@ class FnStats(C.Structure):
     _fields_ = [("cell_overflow", C.c_longlong), ("list_overflow", C.c_longlong),
                 ("rebuilds", C.c_longlong), ("steps", C.c_longlong), ("block_size", C.c_int),
                 ("bond_path", C.c_int), ("n_networks", C.c_int), ("n_beads", C.c_longlong),
-                ("device_bytes", C.c_longlong)]
+                ("device_bytes", C.c_longlong), ("graph_launches", C.c_longlong)]
 
 
 class FnObservables(C.Structure):
     _fields_ = [("reaction", C.c_double * 3), ("broken", C.c_longlong),
                 ("angles_dead", C.c_longlong)]
+
+
+class FnRunInfo(C.Structure):
+    _fields_ = [("run_steps", C.c_int), ("output_freq", C.c_int), ("minimize_steps", C.c_int),
+                ("minimize_substeps", C.c_int), ("minimize_reset", C.c_int),
+                ("export_position", C.c_int), ("export_velocity", C.c_int),
+                ("export_force", C.c_int), ("has_skin_override", C.c_int), ("strict", C.c_int)]
 
 
 # every exported entry point: name -> (restype, argtypes)
@@ -95,6 +102,15 @@ SIGNATURES = {
     "fn_place_fibres": (C.c_int, [C.c_ulonglong, C.c_int, C.c_int, _D, C.c_int, C.c_double,
                                   C.c_double, C.c_double, C.c_int, C.c_double, C.c_double,
                                   C.c_int, _D]),
+    # include/fibrenet_io.h
+    "fn_input_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]),
+    "fn_input_free": (None, [C.c_void_p]),
+    "fn_input_desc": (C.c_int, [C.c_void_p, C.POINTER(FnNetworkDesc)]),
+    "fn_input_info": (C.c_int, [C.c_void_p, C.POINTER(FnRunInfo)]),
+    "fn_input_skin": (C.POINTER(C.c_double), [C.c_void_p]),
+    "fn_input_type_name": (C.c_char_p, [C.c_void_p, C.c_int]),
+    "fn_input_output_stem": (C.c_char_p, [C.c_void_p]),
+    "fn_run_input": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int]),
 }
 
 _lib = None

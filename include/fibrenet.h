@@ -127,6 +127,7 @@ typedef struct fn_stats {
     int n_networks;
     long long n_beads;
     long long device_bytes;    /* device memory held by the context */
+    long long graph_launches;  /* step segments replayed as CUDA graphs */
 } fn_stats;
 
 /* Per-network observables (FP64 reductions on the device). */
@@ -240,8 +241,9 @@ FN_API int fn_forces_only(fn_ctx* ctx, int terms);
 /* Internal bead numbering: perm[internal] = upload index. */
 FN_API int fn_get_permutation(fn_ctx* ctx, int* perm);
 
-/* Time the step kernel at each candidate block size and keep the fastest
-   (state is snapshotted and restored). */
+/* Times steps_per_trial steps at each candidate block size (64 .. 512) from
+   one snapshot of the state, restored after every trial, and keeps the
+   fastest; the simulation does not advance. */
 FN_API int fn_autotune(fn_ctx* ctx, int steps_per_trial);
 
 /* Average duration (ms) of the step kernel over the last fn_step call when

@@ -275,3 +275,36 @@ def test_forces_only_paths(oracle_built, chain):
         s.forces_only(*terms)
         e = rel_norm(s.get("force"), r.get("force"))
         assert e <= FORCE_TOL, (terms, e)
+
+
+def test_graph_replay_is_bit_identical():
+    """Step segments replayed as CUDA graphs give the bits of direct launches,
+    over calls of every length modulo grid_update_freq and both ping-pong
+    parities."""
+    m = g.tensile_network(seed=9, fibres=40, beads=20, box=(40.0, 30.0, 8.0), z_range=(1.0, 7.0),
+                          fail_mu=np.log(0.5), fail_sigma=0.4, clamp_lo=2.0, clamp_hi=38.0,
+                          pull=0.5, cell=2.5)
+    a = sim(m, list_capacity=64, use_graphs=False)
+    b = sim(m, list_capacity=64, use_graphs=True)
+    for n in [1, 2, 7, 8, 9, 16, 17, 3, 8, 5, 24]:
+        a.step(n)
+        b.step(n)
+    for f in FIELDS:
+        np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f)
+    np.testing.assert_array_equal(a.status()[0], b.status()[0])
+    assert b.stats()["graph_launches"] > 0 and a.stats()["graph_launches"] == 0
+
+
+def test_autotune_leaves_state_unchanged():
+    m = g.plain_network(seed=14, fibres=50, beads=20, box=(25.0, 25.0, 6.0), z_range=(1.0, 5.0))
+    a = sim(m, list_capacity=64)
+    b = sim(m, list_capacity=64, use_graphs=True)
+    a.step(13)
+    b.step(13)
+    bs = b.autotune(10)
+    assert bs in (64, 96, 128, 192, 256, 384, 512) and b.stats()["block_size"] == bs
+    assert b.stats()["steps"] == 13
+    a.step(20)
+    b.step(20)
+    for f in FIELDS:
+        np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f)
