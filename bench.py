@@ -254,10 +254,8 @@ def run_e2e(args, m, local, dist, world, nb, barrier):
     torch.cuda.synchronize()
     e2e_wall = time.perf_counter() - w0
     e2e_ms = max(e0.elapsed_time(e1), 1e3 * e2e_wall)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    from fibrenet_b200.ranks import slowest
+    e2e_ms = slowest(e2e_ms, dist, "cuda")
     h2d = sum(getattr(mm, k).nbytes for k in ["pos", "img", "vel", "vel_old", "force", "radius", "mass",
                                             "type", "tag", "loc_id", "s_type", "s_p1", "s_p2",
                                             "s_rest", "s_k", "s_c1", "s_c2", "a_type", "a_b1",
@@ -324,11 +322,9 @@ def run_ours(args):
     kt = sim.kernel_time()
     sim.enable_timing(False)
     barrier()
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-    value = world * nb * args.steps / (elapsed_ms / 1e3)
+    from fibrenet_b200.ranks import job_rate, slowest
+    value = job_rate(nb * args.steps, elapsed_ms, dist, "cuda")
+    elapsed_ms = slowest(elapsed_ms, dist, "cuda")
     stats = sim.stats()
     launches = 1 + args.steps + kt["rebuilds"] * 7
 
@@ -389,10 +385,25 @@ def run_ensemble(args):
 
     from fibrenet_b200 import generate as g
     from fibrenet_b200.native import Simulation
+    from fibrenet_b200.ranks import job_rate, partition_networks, slowest
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
-    ms = g.ensemble_networks(seed=3, n_networks=args.networks)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    all_ms = g.ensemble_networks(seed=3, n_networks=args.networks)
+    # independent networks: split by bead count, no exchange between ranks
+    mine = partition_networks([m.n_beads for m in all_ms], world)[rank]
+    ms = [all_ms[i] for i in mine]
     nb = sum(m.n_beads for m in ms)
+    nb_all = sum(m.n_beads for m in all_ms)
     K = args.steps
 
     def timed(sim, steps):
@@ -407,7 +418,7 @@ def run_ensemble(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    batched = Simulation(ms, list_capacity=32, reorder=True, use_graphs=True)
+    batched = Simulation(ms, device=local, list_capacity=32, reorder=True, use_graphs=True)
     batched.step(max(args.warmup, 3))
     block = batched.autotune(16)
     batched.step(8)
@@ -421,17 +432,26 @@ def run_ensemble(args):
     batched.close()
     t_single = 0.0
     for m in ms:
-        one = Simulation(m, list_capacity=32, reorder=True, use_graphs=True)
+        one = Simulation(m, device=local, list_capacity=32, reorder=True, use_graphs=True)
         one.step(max(args.warmup, 3))
         t_single += timed(one, K)
         one.close()
-    v_b = nb * K / (t_batched / 1e3)
-    v_s = nb * K / (t_single / 1e3)
+    if dist is not None:
+        dist.barrier()
+    v_b = job_rate(nb * K, t_batched, dist, "cuda")
+    v_s = job_rate(nb * K, t_single, dist, "cuda")
+    t_batched = slowest(t_batched, dist, "cuda")
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     line = {"metric": "bead-steps/s (256-network ensemble, batched in one launch per kernel)",
-            "value": v_b, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": max(args.warmup, 3),
-            "ms_per_step": t_batched / K, "higher_is_better": True, "scaling": "weak",
+            "value": v_b, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(args.warmup, 3),
+            "ms_per_step": t_batched / K, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": f"ensemble_{len(ms)}", "networks": len(ms), "beads": nb,
+            "config": {"workload": f"ensemble_{len(all_ms)}", "networks": len(all_ms), "beads": nb_all,
+                       "parallelism": f"networks split over {world} rank(s) by bead count",
                        "fibres_per_network": "U[50, 2000] x 50 beads", "block_size": block,
                        "graphs": True},
             "one_by_one": {"value": v_s, "ms_per_step_all_networks": t_single / K},

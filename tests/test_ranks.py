@@ -1,0 +1,60 @@
+"""Rank logic of the replica / ensemble split, on the CPU with gloo."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from fibrenet_b200.ranks import job_rate, partition_networks, slowest
+
+
+def test_partition_balances_and_covers():
+    counts = [100_000, 2_500, 50_000, 75_000, 30_000, 30_000, 90_000, 10_000]
+    parts = partition_networks(counts, 3)
+    assert sorted(i for p in parts for i in p) == list(range(len(counts)))
+    loads = [sum(counts[i] for i in p) for p in parts]
+    assert max(loads) - min(loads) <= max(counts)
+    assert partition_networks(counts, 1) == [list(range(len(counts)))]
+    with pytest.raises(ValueError):
+        partition_networks(counts, 0)
+
+
+def test_single_process_passthrough():
+    assert slowest(3.5) == 3.5
+    assert job_rate(1000, 500.0) == 2000.0
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # rank r processed (r + 1) * 1000 bead-steps in (r + 1) * 100 ms
+        rate = job_rate((rank + 1) * 1000.0, (rank + 1) * 100.0, dist)
+        out[rank] = (rate, slowest(rank * 7.0, dist))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_aggregate():
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    # (1000 + 2000) bead-steps over the slowest 200 ms
+    assert out[0] == out[1] == (15000.0, 7.0)
