@@ -42,26 +42,53 @@ def parse():
     p.add_argument("--steps", type=int, default=2000)
     p.add_argument("--warmup", type=int, default=40)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--fibres", type=int, default=20000)
+    p.add_argument("--fibres", type=int, default=None,
+                   help="fibre count (default 20,000 tensile / 40,000 dense)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
-    p.add_argument("--workload", choices=["tensile", "ensemble"], default="tensile",
-                   help="tensile: the 1M-bead network (default, the headline); ensemble: 256 "
+    p.add_argument("--workload", choices=["tensile", "dense", "ensemble"], default="tensile",
+                   help="tensile: the 1M-bead network (default, the headline); dense: the 4M-bead "
+                        "periodic 3D mat with penalty + soft-repulsion contacts; ensemble: 256 "
                         "independent networks batched in one context vs run one by one")
     p.add_argument("--networks", type=int, default=256)
-    return p.parse_args()
+    a = p.parse_args()
+    if a.fibres is None:
+        a.fibres = 40000 if a.workload == "dense" else 20000
+    return a
 
 
-def workload(fibres: int):
+def workload(args):
     from fibrenet_b200 import generate as g
-    s = (fibres / 20000.0) ** 0.5
+    if args.workload == "dense":
+        s = (args.fibres / 40000.0) ** (1.0 / 3.0)
+        return g.dense_mat(seed=2, fibres=args.fibres, beads=100, box=(200.0 * s,) * 3)
+    s = (args.fibres / 20000.0) ** 0.5
     box = (1000.0 * s, 1000.0 * s, 20.0)
-    return g.tensile_network(seed=1, fibres=fibres, beads=50, box=box, clamp_lo=2.0,
+    return g.tensile_network(seed=1, fibres=args.fibres, beads=50, box=box, clamp_lo=2.0,
                              clamp_hi=box[0] - 2.0)
 
 
+def metric_for(args):
+    if args.workload == "dense":
+        return "bead-steps/s (dense 3D mat, 1 B200 per replica)"
+    return METRIC
+
+
 def config_dict(m, args, extra=None):
+    if args.workload == "dense":
+        name = "dense_4M" if args.fibres == 40000 else f"dense_{m.n_beads}"
+        d = {"workload": name, "beads": m.n_beads, "springs": m.n_springs, "angles": m.n_angles,
+             "fibres": args.fibres, "beads_per_fibre": 100, "box": list(m.settings.box),
+             "bc": "periodic x,y,z",
+             "contacts": "penalty k 100 on overlap + soft harmonic k 10 below 1.2 (pair kind hsr)",
+             "dt": m.settings.dt, "grid_update_freq": m.settings.grid_update_freq,
+             "cell": m.settings.box_unit_cell, "seed": 2,
+             "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single",
+             "l2": "working set above 126 MB L2 (inputs larger than L2, no flush)"}
+        if extra:
+            d.update(extra)
+        return d
     d = {"workload": WORKLOAD if args.fibres == 20000 else f"tensile_{m.n_beads}",
          "beads": m.n_beads, "springs": m.n_springs, "angles": m.n_angles,
          "fibres": args.fibres, "beads_per_fibre": 50, "box": list(m.settings.box),
@@ -175,10 +202,16 @@ def cpu_reference_rate(model, seconds: float, threads: int | None = None, steps_
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
     m = model.fp32_representable()
-    # the reference has one global boundary type; walls on every axis is the
-    # closest it can express to the finite-x / periodic-y box
-    m.settings.periodic_mask = -1
-    m.settings.bc_type = 1
+    if m.settings.bc_type == 1:
+        # the reference has one global boundary type; walls on every axis is
+        # the closest it can express to the finite-x / periodic-y box
+        m.settings.periodic_mask = -1
+    import numpy as np
+    hsr = np.asarray(m.pair_kind) == 4
+    if hsr.any():
+        # the reference holds one pair kind per type pair: its closest form of
+        # penalty + soft repulsion is the penalty (hs) alone, same lists
+        m.pair_kind = np.where(hsr, 2, m.pair_kind).astype(np.int32)
     kind = "reference"
     if po.ref_available():
         sim = po.RefSim(m, threads=threads)
@@ -203,15 +236,18 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    m = workload(args.fibres)
+    m = workload(args)
     budget = max(30.0, min(150.0, 3.0 * (args.steps + args.warmup)))
     rate, done, threads, kind = cpu_reference_rate(m, budget, steps_cap=args.steps,
                                                    warmup=min(args.warmup, 2))
-    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
+    line = {"metric": metric_for(args), "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
             "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * m.n_beads / rate,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator)", "impl": "reference",
-            "config": config_dict(m, args, {"boundary_in_reference": "walls on all axes"}),
+            "config": config_dict(m, args, {"boundary_in_reference": "walls on all axes"}
+                                  if args.workload == "tensile" else
+                                  {"contacts_in_reference": "hs penalty k 100 only (one pair kind "
+                                                            "per type pair in the reference)"}),
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": f"{done} whole steps of the full {m.n_beads}-bead network "
                                        f"(time-bounded, {budget:.0f} s)"},
@@ -245,7 +281,7 @@ def run_e2e(args, m, local, dist, world, nb, barrier):
     while done < e2e_steps:
         k = min(OUTPUT_FREQ, e2e_steps - done)
         sim2.step(k)
-        o = sim2.observe(0, reaction_type=2)
+        o = sim2.observe(0, reaction_type=2 if m.n_types > 2 else -1)
         obs_bytes += 5 * 8
         done += k
     final = sim2.get("pos")
@@ -289,7 +325,7 @@ def run_ours(args):
 
     from fibrenet_b200.native import Simulation
 
-    m = workload(args.fibres)
+    m = workload(args)
     sim = Simulation(m, device=local, list_capacity=64, cell_capacity=64, reorder=True)
     nb = m.n_beads
 
@@ -346,11 +382,12 @@ def run_ours(args):
         rate, done_cpu, threads, kind = cpu_reference_rate(m, args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{done_cpu} whole steps of the same {nb}-bead network on the host "
-                         f"(reference kernels as C, OpenMP, walls on all axes)"}
+                         f"(reference kernels as C, OpenMP, "
+                         f"{'walls on all axes' if args.workload == 'tensile' else 'hs penalty only'})"}
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": metric_for(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator; reference ships no models)",

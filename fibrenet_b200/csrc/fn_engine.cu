@@ -316,6 +316,10 @@ void pair_coeffs(int kind, const double* raw, FnPair& P) {
         P.c[3] = 48.0 * epsilon * fr6 * (fr6 - 0.5) / r2;
     } else if (kind == FN_PAIR_HS) {
         P.c[0] = raw[0];
+    } else if (kind == FN_PAIR_HSR) {
+        P.c[0] = raw[0];
+        P.c[1] = raw[1];
+        P.c[2] = raw[2];
     } else if (kind == FN_PAIR_ST) {
         P.c[0] = raw[1];
         P.c[1] = raw[2];
@@ -846,9 +850,12 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         for (int p = 0; p < npairs; ++p) {
             FnPair P;
             pair_coeffs(d.pair_kind[p], d.pair_raw + 4 * p, P);
+            if (P.kind == FN_PAIR_HSR && !(P.c[2] <= d.settings.cutoff))
+                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) +
+                                               ": hsr soft radius exceeds the cutoff (pairs would go unlisted)");
             c->pairs_h.push_back(P);
-            any_cut |= P.kind == FN_PAIR_LJ || P.kind == FN_PAIR_ST;
-            any_hs |= P.kind == FN_PAIR_HS;
+            any_cut |= P.kind == FN_PAIR_LJ || P.kind == FN_PAIR_ST || P.kind == FN_PAIR_HSR;
+            any_hs |= P.kind == FN_PAIR_HS || P.kind == FN_PAIR_HSR;
         }
         /* largest listing radius (squared): cutoff for lj/st, the largest
            radius + the largest skin for hs (kernel.cl:632-650) */

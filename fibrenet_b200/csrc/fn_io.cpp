@@ -247,6 +247,9 @@ void types_pairs(const Lines& t, fn_input& in) {
         } else if (tk[1] == "st") {
             kind = FN_PAIR_ST;
             want = 8;
+        } else if (tk[1] == "hsr") {
+            kind = FN_PAIR_HSR; /* extension: K k rc */
+            want = 7;
         } else {
             fail("line %d: unknown interaction type '%s'", l, tk[1].c_str());
         }

@@ -201,6 +201,29 @@ __device__ __forceinline__ int contact_eval(const FnNet& N, const FnPair* __rest
         }
         return 0;
     }
+    if (kind == 4) {
+        /* extension, no counterpart in the reference: penalty spring K (c1)
+           on the overlap plus a soft harmonic repulsion k (c2) below rc (c3) */
+        length = sqrt(length);
+        const double penetration = ((double)w_radius(pi.w) + (double)w_radius(pj.w)) - length;
+        double mag = 0.0;
+        int acts = 0;
+        if (penetration > 0.0) {
+            mag += penetration * P->c[0];
+            acts = 1;
+        }
+        if (length < P->c[2]) {
+            mag += (P->c[2] - length) * P->c[1];
+            acts = 1;
+        }
+        if (acts) {
+            length = (length != 0.0) ? 1.0 / length : 0.0;
+            Rx = mag * (rx * length);
+            Ry = mag * (ry * length);
+            Rz = mag * (rz * length);
+        }
+        return acts;
+    }
     if (kind == 3) {
         if (length < P->c[3]) {
             length = sqrt(length);
@@ -944,7 +967,8 @@ __device__ __forceinline__ bool list_accept(const FnNet& N, const FnPair* __rest
     if (bi.x == bj.x && abs(bi.y - bj.y) <= 1) return false;
     const int kind = pairs[N.pair_base + getadress(bi.z, bj.z, N.types_num)].kind;
     if (kind == 1 || kind == 3) return length < N.cutoff_sq;
-    if (kind == 2) {
+    if (kind == 2 || kind == 4) {
+        if (kind == 4 && length < N.cutoff_sq) return true;
         const double si = (double)__int_as_float(bi.w), sj = (double)__int_as_float(bj.w);
         const double ri = (double)w_radius(pi.w), rj = (double)w_radius(pj.w);
         const double min_skin = (si > sj) ? sj : si;

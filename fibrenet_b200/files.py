@@ -12,10 +12,10 @@ import os
 
 import numpy as np
 
-from .model import PAIR_HS, PAIR_LJ, PAIR_ST, Model, Settings, pair_index
+from .model import PAIR_HS, PAIR_HSR, PAIR_LJ, PAIR_ST, Model, Settings, pair_index
 
-PAIR_NAMES = {PAIR_LJ: "lj", PAIR_HS: "hs", PAIR_ST: "st"}
-PAIR_TOKENS = {PAIR_LJ: 3, PAIR_HS: 1, PAIR_ST: 4}
+PAIR_NAMES = {PAIR_LJ: "lj", PAIR_HS: "hs", PAIR_ST: "st", PAIR_HSR: "hsr"}
+PAIR_TOKENS = {PAIR_LJ: 3, PAIR_HS: 1, PAIR_ST: 4, PAIR_HSR: 3}
 
 
 def _g(x) -> str:

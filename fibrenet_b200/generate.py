@@ -371,3 +371,23 @@ def ensemble_networks(seed=3, n_networks=256, fibres_lo=50, fibres_hi=2000, bead
         m.meta.update(kind="ensemble", index=k, k_s=ks, k_a=ka)
         out.append(m)
     return out
+
+
+def dense_mat(seed=2, fibres=40000, beads=100, box=(200.0, 200.0, 200.0), k_s=200.0, k_a=5.0,
+              k_pen=100.0, k_soft=10.0, rc_soft=1.2, vel_sigma=0.1, dt=0.0005, cell=1.0,
+              cutoff=1.2, grid_update_freq=8) -> Model:
+    """Dense 3D mat (config 2 at its default sizes): periodic 200^3 box, fibres
+    of 100 beads with directions uniform on the sphere, HR springs (rest 1,
+    k 200) and angles (k 5), contacts = penalty (k 100) + soft harmonic
+    repulsion (k 10 below 1.2) on the same type pair (pair kind 4, an
+    extension), Gaussian velocities (sigma 0.1)."""
+    from .model import PAIR_HSR
+    rng = np.random.default_rng(seed)
+    pts = place_fibres(rng, fibres, beads, box, (True, True, True), orient="sphere")
+    st = Settings(dt=dt, lam=0.5, damping=0.0, cutoff=cutoff, box_unit_cell=cell, box=tuple(box),
+                  wall_k=0.0, bc_type=0, grid_update_freq=grid_update_freq)
+    pk, pr = _uniform_pairs(1, PAIR_HSR, [k_pen, k_soft, rc_soft, 0])
+    vel = rng.normal(0.0, vel_sigma, (fibres * beads, 3))
+    m = chain_model(pts, st, ["C1"], pk, pr, k_s=k_s, k_a=k_a, vel=vel)
+    m.meta.update(kind="dense", seed=seed, fibres=fibres, beads=beads)
+    return m

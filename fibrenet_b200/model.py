@@ -18,6 +18,7 @@ import numpy as np
 PAIR_LJ = 1
 PAIR_HS = 2
 PAIR_ST = 3
+PAIR_HSR = 4  # extension: penalty + soft harmonic repulsion on one type pair
 
 SPRING_HR = 0
 SPRING_HR_FL = 1

@@ -43,8 +43,11 @@ enum {
     FN_VELOCITY_OLD = 4   /* Bead.velocity_old */
 };
 
-/* pair kinds (SimulationManager.cpp:891-932) */
-enum { FN_PAIR_LJ = 1, FN_PAIR_HS = 2, FN_PAIR_ST = 3 };
+/* pair kinds (SimulationManager.cpp:891-932); FN_PAIR_HSR is an extension
+   without reference counterpart: penalty K plus a soft harmonic repulsion k
+   below rc on one type pair (raw tokens K, k, rc; listed within the hs
+   radius or the cutoff) */
+enum { FN_PAIR_LJ = 1, FN_PAIR_HS = 2, FN_PAIR_ST = 3, FN_PAIR_HSR = 4 };
 
 typedef struct fn_ctx fn_ctx;
 

@@ -478,6 +478,28 @@ static int contact_force(const fo_ctx* c, int i, int j, int pair_id, double R[3]
         }
         return 0;
     }
+    if (kind == 4) {
+        /* extension without reference counterpart (penalty + soft repulsion) */
+        length = sqrt(length);
+        double penetration = (c->radius[i] + c->radius[j]) - length;
+        double mag = 0.0;
+        int acts = 0;
+        if (penetration > 0.0) {
+            mag += penetration * cc[0];
+            acts = 1;
+        }
+        if (length < cc[2]) {
+            mag += (cc[2] - length) * cc[1];
+            acts = 1;
+        }
+        if (acts) {
+            length = (length != 0.0) ? 1.0 / length : 0.0;
+            R[0] = mag * (rij[0] * length);
+            R[1] = mag * (rij[1] * length);
+            R[2] = mag * (rij[2] * length);
+        }
+        return acts;
+    }
     if (kind == 3) {
         if (length < cc[3]) {
             length = sqrt(length);
@@ -514,10 +536,10 @@ static int list_candidate(const fo_ctx* c, int b1, int b2) {
     if (c->list_mi) length = min_image(c, rij, length, c->list_mi);
     int pair_id = getadress(c->type[b1], c->type[b2], c->d.types_num);
     int kind = c->p_kind[pair_id];
-    if (kind == 1 || kind == 3) {
+    if (kind == 1 || kind == 3 || kind == 4) {
         if (length < c->d.cutoff_sq) return pair_id;
     }
-    if (kind == 2) {
+    if (kind == 2 || kind == 4) {
         double min_skin = (c->skin[b1] > c->skin[b2]) ? c->skin[b2] : c->skin[b1];
         double max_radius = (c->radius[b1] > c->radius[b2]) ? c->radius[b1] : c->radius[b2];
         double lim = max_radius + min_skin;

@@ -94,6 +94,10 @@ static inline void fo_derive_pair(int kind, const double raw[4], double c[6]) {
         c[3] = fpr;
     } else if (kind == 2) {
         c[0] = raw[0];
+    } else if (kind == 4) { /* extension: penalty K, soft k, rc (no reference counterpart) */
+        c[0] = raw[0];
+        c[1] = raw[1];
+        c[2] = raw[2];
     } else if (kind == 3) {
         c[0] = raw[1];
         c[1] = raw[2];

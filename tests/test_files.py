@@ -153,3 +153,11 @@ def test_restart_file_is_read(tmp):
     np.testing.assert_array_equal(r.pos, pos)
     np.testing.assert_array_equal(r.img, pos + 1)
     np.testing.assert_array_equal(r.vel_old, vel)
+
+
+def test_hsr_pair_keyword_round_trip(tmp):
+    """The penalty + soft-repulsion kind (an extension, 'pair hsr T1 T2 K k rc')."""
+    m = g.dense_mat(fibres=6, beads=8, box=(12.0, 12.0, 12.0))
+    r, _, _ = files.read_input(write(m, tmp), strict=True)
+    assert r.pair_kind.tolist() == [4]
+    np.testing.assert_array_equal(r.pair_raw[0, :3], [100.0, 10.0, 1.2])
