@@ -123,6 +123,8 @@ struct fn_ctx {
     DevBuf<FnPair> pairs;
     DevBuf<unsigned long long> counters;
     DevBuf<double> obs_partial, obs_out;
+    DevBuf<double> en_partial, en_out;
+    DevBuf<double> series; /* rows of fn_step_series */
     int list_stride = 0;
     int cur = 0;
     int block = 128;
@@ -240,6 +242,9 @@ void free_all(fn_ctx* c) {
     dfree(c, c->counters);
     dfree(c, c->obs_partial);
     dfree(c, c->obs_out);
+    dfree(c, c->en_partial);
+    dfree(c, c->en_out);
+    dfree(c, c->series);
 }
 
 /* Kernel constants of one network (SimulationManager.cpp:647-671, 684-720,
@@ -1041,6 +1046,8 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     CK(dalloc(c, c->counters, FN_CNT_N));
     CK(dalloc(c, c->obs_partial, 5 * 1024));
     CK(dalloc(c, c->obs_out, 8));
+    CK(dalloc(c, c->en_partial, (size_t)fn::FN_EN_N * 1024));
+    CK(dalloc(c, c->en_out, fn::FN_EN_N));
 
     c->cur = 0;
     CK(h2d(c, c->pos[0], pos));
@@ -1334,11 +1341,10 @@ FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_s
     return FN_OK;
 }
 
-FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out) {
-    int r = check_ready(c);
-    if (r) return r;
-    if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_observe: bad arguments");
-    CK(cudaSetDevice(c->cfg.device));
+namespace {
+
+/* Observables of network `net` into out[0..4] on the context's stream. */
+int observe_async(fn_ctx* c, int net, int reaction_type, double* out) {
     const NetHost& h = c->info[net];
     fn::ObserveArgs O{};
     O.ch_flags = c->chain ? c->ch_flags.p : nullptr;
@@ -1358,13 +1364,119 @@ FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out
     long long span = std::max({(long long)(h.bead_end - h.bead_begin), (long long)(h.spring_end - h.spring_begin),
                                (long long)(h.angle_end - h.angle_begin), 1LL});
     int nblocks = (int)std::min<long long>(1024, (span + 255) / 256);
-    CK(fn::launch_observe(O, nblocks, c->obs_out.p, c->stream));
+    CK(fn::launch_observe(O, nblocks, out, c->stream));
+    return FN_OK;
+}
+
+/* Energy and virial of network `net` into out[0..FN_EN_N) on the stream. */
+int energy_async(fn_ctx* c, int net, double* out) {
+    const NetHost& h = c->info[net];
+    fn::EnergyArgs E{};
+    E.nets = c->nets.p;
+    E.pairs = c->pairs.p;
+    E.pos = c->pos[c->cur].p;
+    E.img = c->img[c->cur].p;
+    E.vold = c->vold.p;
+    E.sp_ends = c->sp_ends.p;
+    E.sp_par = c->sp_par.p;
+    E.sp_type = c->sp_type.p;
+    E.sp_status = c->sp_status.p;
+    E.an_b = c->an_b.p;
+    E.an_par = c->an_par.p;
+    E.an_status = c->an_status.p;
+    E.ch_status = c->chain ? c->ch_status.p : nullptr;
+    E.list_count = c->list_count.p;
+    E.list = c->list.p;
+    E.list_stride = c->list_stride;
+    E.list_cap = c->cfg.list_capacity;
+    E.net = net;
+    E.bead_begin = h.bead_begin;
+    E.bead_end = h.bead_end;
+    E.spring_begin = h.spring_begin;
+    E.spring_end = h.spring_end;
+    E.angle_begin = h.angle_begin;
+    E.angle_end = h.angle_end;
+    E.partial = c->en_partial.p;
+    long long span = std::max({(long long)(h.bead_end - h.bead_begin), (long long)(h.spring_end - h.spring_begin),
+                               (long long)(h.angle_end - h.angle_begin), 1LL});
+    int nblocks = (int)std::min<long long>(1024, (span + 255) / 256);
+    CK(fn::launch_energy(E, nblocks, out, c->stream));
+    return FN_OK;
+}
+
+}  // namespace
+
+FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_observe: bad arguments");
+    CK(cudaSetDevice(c->cfg.device));
+    r = observe_async(c, net, reaction_type, c->obs_out.p);
+    if (r) return r;
     double res[5];
     CK(cudaMemcpyAsync(res, c->obs_out.p, sizeof res, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (int a = 0; a < 3; ++a) out->reaction[a] = res[a];
     out->broken = (long long)res[3];
     out->angles_dead = (long long)res[4];
+    return FN_OK;
+}
+
+
+FN_API int fn_energy_eval(fn_ctx* c, int net, fn_energy* out) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_energy_eval: bad arguments");
+    CK(cudaSetDevice(c->cfg.device));
+    r = energy_async(c, net, c->en_out.p);
+    if (r) return r;
+    double res[fn::FN_EN_N];
+    CK(cudaMemcpyAsync(res, c->en_out.p, sizeof res, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->kinetic = res[fn::FN_EN_KINETIC];
+    out->spring = res[fn::FN_EN_SPRING];
+    out->angle = res[fn::FN_EN_ANGLE];
+    out->contact = res[fn::FN_EN_CONTACT];
+    out->wall = res[fn::FN_EN_WALL];
+    out->gravity = res[fn::FN_EN_GRAVITY];
+    for (int k = 0; k < 9; ++k) out->virial[k] = res[fn::FN_EN_VIRIAL + k];
+    out->contacts = (long long)res[fn::FN_EN_CONTACTS];
+    return FN_OK;
+}
+
+FN_API int fn_step_series(fn_ctx* c, int nsteps, int every, int net, int reaction_type,
+                          int with_energy, double* host_rows) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (nsteps <= 0 || every <= 0 || net < 0 || net >= c->n_nets || !host_rows)
+        return fail(c, FN_ERR_ARG, "fn_step_series: bad arguments");
+    CK(cudaSetDevice(c->cfg.device));
+    const int width = with_energy ? 6 + fn::FN_EN_N : 6;
+    const long long rows = (nsteps + (long long)every - 1) / every;
+    const size_t need = (size_t)rows * width;
+    if (c->series.n < need) {
+        dfree(c, c->series);
+        CK(dalloc(c, c->series, need));
+    }
+    std::vector<double> steps_done(rows);
+    int done = 0;
+    for (long long q = 0; q < rows; ++q) {
+        const int k = std::min(every, nsteps - done);
+        r = fn_step(c, k);
+        if (r) return r;
+        done += k;
+        double* row = c->series.p + (size_t)q * width;
+        r = observe_async(c, net, reaction_type, row + 1);
+        if (r) return r;
+        if (with_energy) {
+            r = energy_async(c, net, row + 6);
+            if (r) return r;
+        }
+        steps_done[q] = (double)done;
+    }
+    CK(cudaMemcpyAsync(host_rows, c->series.p, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (long long q = 0; q < rows; ++q) host_rows[(size_t)q * width] = steps_done[q];
     return FN_OK;
 }
 

@@ -1373,6 +1373,184 @@ cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, 
     return cudaGetLastError();
 }
 
+/* ---------------------------------------------------------------------------
+   Energy and virial (an addition: the reference computes neither).  Each term
+   is the potential whose negative gradient is the force the step applies:
+     spring   k/2 (L - L0)^2                      (F = k (L0 - L) u)
+     angle    k (theta - theta0)^2                (M = -2 k (theta - theta0))
+     hs       K/2 p^2, p = r_i + r_j - r > 0
+     hsr      K/2 p^2 + k/2 (rc - r)^2 for r < rc
+     lj       48 eps s^12/13 (r^-13 - rc^-13) - 24 eps s^6/7 (r^-7 - rc^-7)
+              + c4 (r - rc), the integral of the shifted force to rc = c3
+     st       K (c2 (rc - r) - (rc^2 - r^2)/2) + K0 (c6 (rc - r) - (rc^2 - r^2)/2)
+     wall     wall_k/2 d^2 for a penetration d past a wall
+     gravity  -g . x (image position; g is a force per bead)
+   Kinetic energy is m/2 |v|^2 of the step-end velocity (velocity_old) over
+   beads of non-zero mass.  The virial is sum r_ij (x) F_ij over springs,
+   angles (r_ba (x) F_a + r_bc (x) F_c) and contact pairs, each pair once. */
+__device__ __forceinline__ double contact_energy(const FnNet& N, const FnPair* __restrict__ pairs,
+                                                 double4 pi, double4 pj, double& Rx, double& Ry,
+                                                 double& Rz, double& rx, double& ry, double& rz,
+                                                 int& acts) {
+    rx = pi.x - pj.x;
+    ry = pi.y - pj.y;
+    rz = pi.z - pj.z;
+    double r2 = rx * rx + ry * ry + rz * rz;
+    r2 = min_image(N, rx, ry, rz, r2, N.force_mi);
+    acts = contact_eval(N, pairs, pi, pj, Rx, Ry, Rz);
+    if (!acts) return 0.0;
+    const FnPair* P = pairs + N.pair_base + getadress(w_type(pi.w), w_type(pj.w), N.types_num);
+    const double r = sqrt(r2);
+    const double rsum = (double)w_radius(pi.w) + (double)w_radius(pj.w);
+    switch (P->kind) {
+    case 1: {
+        const double rc = P->c[2], s2 = P->c[0] * P->c[0], eps = P->c[1];
+        const double s6 = s2 * s2 * s2, s12 = s6 * s6;
+        const double ir = 1.0 / r, irc = 1.0 / rc;
+        const double ir7 = pow(ir, 7.0), ir13 = pow(ir, 13.0);
+        const double irc7 = pow(irc, 7.0), irc13 = pow(irc, 13.0);
+        return 48.0 * eps * s12 / 13.0 * (ir13 - irc13) - 24.0 * eps * s6 / 7.0 * (ir7 - irc7) +
+               P->c[3] * (r - rc);
+    }
+    case 2: {
+        const double p = rsum - r;
+        return 0.5 * P->c[0] * p * p;
+    }
+    case 3: {
+        const double rc = sqrt(P->c[3]);
+        const double q = 0.5 * (rc * rc - r * r);
+        return P->c[0] * (P->c[1] * (rc - r) - q) + P->c[4] * (P->c[5] * (rc - r) - q);
+    }
+    case 4: {
+        const double p = rsum - r;
+        double u = p > 0.0 ? 0.5 * P->c[0] * p * p : 0.0;
+        if (r < P->c[2]) u += 0.5 * P->c[1] * (P->c[2] - r) * (P->c[2] - r);
+        return u;
+    }
+    }
+    return 0.0;
+}
+
+__device__ __forceinline__ void add_outer(double* w, double ax, double ay, double az, double bx,
+                                          double by, double bz) {
+    w[0] += ax * bx;
+    w[1] += ax * by;
+    w[2] += ax * bz;
+    w[3] += ay * bx;
+    w[4] += ay * by;
+    w[5] += ay * bz;
+    w[6] += az * bx;
+    w[7] += az * by;
+    w[8] += az * bz;
+}
+
+__global__ void __launch_bounds__(256) k_energy_partial(const EnergyArgs E) {
+    __shared__ double red[256];
+    const FnNet N = E.nets[E.net];
+    double acc[FN_EN_N];
+#pragma unroll
+    for (int k = 0; k < FN_EN_N; ++k) acc[k] = 0.0;
+    double* W = acc + FN_EN_VIRIAL;
+    const int stride = gridDim.x * blockDim.x;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+
+    for (int i = E.bead_begin + t0; i < E.bead_end; i += stride) {
+        const double4 p = E.pos[i];
+        const double4 im = E.img[i];
+        if (im.w > 0.0) {
+            const float4 v = E.vold[i];
+            const double vx = v.x, vy = v.y, vz = v.z;
+            acc[FN_EN_KINETIC] += 0.5 / im.w * (vx * vx + vy * vy + vz * vz);
+        }
+        acc[FN_EN_GRAVITY] -= N.g[0] * im.x + N.g[1] * im.y + N.g[2] * im.z;
+        if (N.walls) {
+            const double pc[3] = {p.x, p.y, p.z};
+            for (int a = 0; a < 3; ++a) {
+                if (!(N.walls & (1 << a))) continue;
+                double d = 0.0;
+                if (pc[a] < 0.0) d = pc[a];
+                if (pc[a] > N.box[a]) d = pc[a] - N.box[a];
+                acc[FN_EN_WALL] += 0.5 * N.wall_k * d * d;
+            }
+        }
+        int n = E.list_count[i];
+        if (n > E.list_cap) n = E.list_cap;
+        for (int k = 0; k < n; ++k) {
+            const int j = E.list[(size_t)k * E.list_stride + i];
+            if (j <= i) continue;
+            double Rx, Ry, Rz, rx, ry, rz;
+            int acts;
+            const double u = contact_energy(N, E.pairs, p, E.pos[j], Rx, Ry, Rz, rx, ry, rz, acts);
+            if (acts) {
+                acc[FN_EN_CONTACT] += u;
+                acc[FN_EN_CONTACTS] += 1.0;
+                add_outer(W, rx, ry, rz, Rx, Ry, Rz);
+            }
+        }
+    }
+    for (int s = E.spring_begin + t0; s < E.spring_end; s += stride) {
+        const int type = E.sp_type[s];
+        if (!(type == 0 || type == 1)) continue;
+        const int2 e = E.sp_ends[s];
+        const int alive = E.ch_status ? (E.ch_status[min(e.x, e.y)] & 1) : (E.sp_status[s] == 1);
+        if (!alive) continue;
+        const double4 a = E.img[e.x], b = E.img[e.y];
+        const float4 par = E.sp_par[s];
+        double fx, fy, fz;
+        int broke;
+        spring_pts(a.x, a.y, a.z, b.x, b.y, b.z, par, 0, fx, fy, fz, broke);
+        const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+        const double L = sqrt(dx * dx + dy * dy + dz * dz) - (double)par.x;
+        acc[FN_EN_SPRING] += 0.5 * (double)par.y * L * L;
+        add_outer(W, dx, dy, dz, fx, fy, fz);
+    }
+    for (int q = E.angle_begin + t0; q < E.angle_end; q += stride) {
+        const int4 b = E.an_b[q];
+        const int alive = E.ch_status ? ((E.ch_status[b.y] >> 1) & 1) : (E.an_status[q] == 1);
+        if (!alive) continue;
+        const double4 t1 = E.img[b.x], t2 = E.img[b.y], t3 = E.img[b.z];
+        const float2 par = E.an_par[q];
+        double pax, pay, paz, pcx, pcy, pcz;
+        angle_pts(t1.x, t1.y, t1.z, t2.x, t2.y, t2.z, t3.x, t3.y, t3.z, par, pax, pay, paz, pcx,
+                  pcy, pcz);
+        const double bax = t1.x - t2.x, bay = t1.y - t2.y, baz = t1.z - t2.z;
+        const double bcx = t3.x - t2.x, bcy = t3.y - t2.y, bcz = t3.z - t2.z;
+        double dotp = (bax * bcx + bay * bcy + baz * bcz) /
+                      (sqrt(bax * bax + bay * bay + baz * baz) * sqrt(bcx * bcx + bcy * bcy + bcz * bcz));
+        if (dotp < -1.0) dotp = -0.999999;
+        if (dotp > 1.0) dotp = 0.999999;
+        const double d = fn_acos(dotp) - (double)par.x;
+        acc[FN_EN_ANGLE] += (double)par.y * d * d;
+        add_outer(W, bax, bay, baz, pax, pay, paz);
+        add_outer(W, bcx, bcy, bcz, pcx, pcy, pcz);
+    }
+    /* fixed-order block reduction, one quantity at a time */
+    for (int k = 0; k < FN_EN_N; ++k) {
+        red[threadIdx.x] = acc[k];
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) E.partial[(size_t)FN_EN_N * blockIdx.x + k] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_energy_final(const double* partial, int nblocks, double* out) {
+    const int k = threadIdx.x;
+    if (blockIdx.x != 0 || k >= FN_EN_N) return;
+    double a = 0.0;
+    for (int b = 0; b < nblocks; ++b) a += partial[(size_t)FN_EN_N * b + k];
+    out[k] = a;
+}
+
+cudaError_t launch_energy(const EnergyArgs& E, int nblocks, double* out, cudaStream_t s) {
+    k_energy_partial<<<nblocks, 256, 0, s>>>(E);
+    k_energy_final<<<1, 32, 0, s>>>(E.partial, nblocks, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_observe(const ObserveArgs& O, int nblocks, double* out, cudaStream_t s) {
     k_observe_partial<<<nblocks, 256, 0, s>>>(O);
     k_observe_final<<<1, 32, 0, s>>>(O.partial, nblocks, out);

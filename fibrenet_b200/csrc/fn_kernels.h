@@ -155,6 +155,37 @@ struct ObserveArgs {
     double* partial; /* 5 doubles per block */
 };
 
+/* energy and virial of one network (not part of the reference): FP64 sums
+   over beads, springs, angles and contact pairs i < j */
+enum { FN_EN_KINETIC, FN_EN_SPRING, FN_EN_ANGLE, FN_EN_CONTACT, FN_EN_WALL, FN_EN_GRAVITY,
+       FN_EN_VIRIAL, FN_EN_CONTACTS = FN_EN_VIRIAL + 9, FN_EN_N };
+
+struct EnergyArgs {
+    const FnNet* nets;
+    const FnPair* pairs;
+    const double4* pos;
+    const double4* img;
+    const float4* vold;
+    const int2* sp_ends;
+    const float4* sp_par;
+    const signed char* sp_type;
+    const signed char* sp_status;
+    const int4* an_b;
+    const float2* an_par;
+    const signed char* an_status;
+    const unsigned char* ch_status; /* chain form: statuses per bead, else null */
+    const int* list_count;
+    const int* list;
+    int list_stride, list_cap;
+    int net;
+    int bead_begin, bead_end;
+    int spring_begin, spring_end;
+    int angle_begin, angle_end;
+    double* partial; /* FN_EN_N doubles per block */
+};
+
+cudaError_t launch_energy(const EnergyArgs& E, int nblocks, double* out, cudaStream_t s);
+
 cudaError_t launch_step(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
                         bool store_v, cudaStream_t s);
 cudaError_t launch_step_tiled(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,

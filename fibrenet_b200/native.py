@@ -62,6 +62,17 @@ class FnObservables(C.Structure):
                 ("angles_dead", C.c_longlong)]
 
 
+class FnEnergy(C.Structure):
+    _fields_ = [("kinetic", C.c_double), ("spring", C.c_double), ("angle", C.c_double),
+                ("contact", C.c_double), ("wall", C.c_double), ("gravity", C.c_double),
+                ("virial", C.c_double * 9), ("contacts", C.c_longlong)]
+
+
+ENERGY_FIELDS = ["kinetic", "spring", "angle", "contact", "wall", "gravity"]
+SERIES_COLUMNS = (["step", "reaction_x", "reaction_y", "reaction_z", "broken", "angles_dead"]
+                  + ENERGY_FIELDS + [f"virial_{a}{b}" for a in "xyz" for b in "xyz"] + ["contacts"])
+
+
 class FnRunInfo(C.Structure):
     _fields_ = [("run_steps", C.c_int), ("output_freq", C.c_int), ("minimize_steps", C.c_int),
                 ("minimize_substeps", C.c_int), ("minimize_reset", C.c_int),
@@ -90,6 +101,8 @@ SIGNATURES = {
     "fn_observe": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(FnObservables)]),
     "fn_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FnStats)]),
     "fn_observe_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "fn_energy_eval": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FnEnergy)]),
+    "fn_step_series": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _D]),
     "fn_get_cells": (C.c_int, [C.c_void_p, _I, _I, C.c_longlong]),
     "fn_get_lists": (C.c_int, [C.c_void_p, _I, _I, C.c_int]),
     "fn_n_cells": (C.c_longlong, [C.c_void_p]),
@@ -292,6 +305,28 @@ class Simulation:
         asynchronously; call sync() before reading it."""
         self._check(self.lib.fn_observe_noalloc(self.h, net, reaction_type,
                                                 C.c_void_p(out_device_ptr)))
+
+    def energy(self, net: int = 0) -> dict:
+        """Energy terms, their sum ("total"), the 3x3 virial and the count of
+        acting contact pairs of network ``net`` (fn_energy_eval)."""
+        e = FnEnergy()
+        self._check(self.lib.fn_energy_eval(self.h, net, C.byref(e)))
+        out = {f: float(getattr(e, f)) for f in ENERGY_FIELDS}
+        out["total"] = sum(out[f] for f in ENERGY_FIELDS)
+        out["virial"] = np.array(e.virial[:]).reshape(3, 3)
+        out["contacts"] = int(e.contacts)
+        return out
+
+    def step_series(self, nsteps: int, every: int, net: int = 0, reaction_type: int = -1,
+                    energy: bool = False) -> np.ndarray:
+        """Runs nsteps in chunks of ``every`` and returns one row per chunk
+        (columns SERIES_COLUMNS[:6], or all 22 with ``energy``)."""
+        width = len(SERIES_COLUMNS) if energy else 6
+        rows = -(-nsteps // every)
+        out = np.zeros((rows, width), np.float64)
+        self._check(self.lib.fn_step_series(self.h, nsteps, every, net, reaction_type, int(energy),
+                                            out.ctypes.data_as(_D)))
+        return out
 
     def stats(self) -> dict:
         s = FnStats()

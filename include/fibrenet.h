@@ -140,6 +140,21 @@ typedef struct fn_observables {
     long long angles_dead;/* angles with status 0 */
 } fn_observables;
 
+/* Energy and virial of one network (FP64 device reductions; the reference
+   computes neither).  Each potential is the one whose negative gradient is the
+   force the step applies: springs k/2 (L - L0)^2, angles k (theta - theta0)^2,
+   hs K/2 p^2 (p = overlap), hsr K/2 p^2 + k/2 (rc - r)^2 below rc, lj and st
+   the integrals of their (shifted) forces out to their cut-off, walls
+   wall_k/2 d^2, gravity -g.x on image positions.  kinetic = m/2 |v|^2 of the
+   step-end velocity (velocity_old) over beads of non-zero mass.  virial =
+   sum r_ij (x) F_ij over springs, angles and contact pairs (row-major 3x3,
+   r in minimum image for contacts, image positions for bonds). */
+typedef struct fn_energy {
+    double kinetic, spring, angle, contact, wall, gravity;
+    double virial[9];
+    long long contacts; /* contact pairs with a non-zero force */
+} fn_energy;
+
 /* OpenclManager::Initialize (OpenclManager.cpp:5-85) without the interactive
    platform/device prompt: binds cfg->device and creates the stream. */
 FN_API int fn_create(const fn_config* cfg, fn_ctx** out);
@@ -209,6 +224,20 @@ FN_API int fn_set_status(fn_ctx* ctx, const int* spring_status, const int* angle
 FN_API int fn_observe(fn_ctx* ctx, int net, int reaction_type, fn_observables* out);
 
 FN_API int fn_get_stats(fn_ctx* ctx, fn_stats* out);
+
+/* Energy and virial of network `net` at the current state (after fn_step the
+   state holds the positions its last forces were evaluated at). */
+FN_API int fn_energy_eval(fn_ctx* ctx, int net, fn_energy* out);
+
+/* The Run flow's time series without a host round trip per chunk: runs
+   nsteps as fn_step(every) calls (the rebuild counter restarts with every
+   chunk, SimulationManager.cpp:152) and after each chunk records, on the
+   device, one row for network `net`: {steps done, reaction x, y, z, broken
+   springs, dead angles} and, when with_energy != 0, the 16 fields of
+   fn_energy (contacts as a double).  Rows are copied to host_rows
+   (ceil(nsteps / every) rows of 6 or 22 doubles) once, at the end. */
+FN_API int fn_step_series(fn_ctx* ctx, int nsteps, int every, int net, int reaction_type,
+                          int with_energy, double* host_rows);
 
 /* The observables of fn_observe for callers that cannot allocate device
    memory when they need them, e.g. code that runs while a CUDA graph is being
