@@ -14,10 +14,7 @@ import pytest
 
 import energy_ref as er
 from fibrenet_b200 import generate as g
-from fibrenet_b200.model import PAIR_HSR, PAIR_LJ, PAIR_ST
-
-INTERNAL = ("spring", "angle", "contact")
-
+from fibrenet_b200.model import PAIR_ST
 
 def perturbed(m, sigma, seed=0):
     rng = np.random.default_rng(seed)
@@ -144,7 +141,7 @@ def test_energy_matches_numpy(kind, chain):
     with sim(m, chain=chain) as s:
         s.step(25)
         e = check_against_numpy(s, m)
-    assert e["contact"] > 0.0 and e["kinetic"] > 0.0
+    assert e["contact"] != 0.0 and e["kinetic"] > 0.0  # lj contact energy is negative
 
 
 @pytest.mark.gpu
@@ -161,11 +158,14 @@ def test_energy_of_each_network_in_a_batch():
 
 @pytest.mark.gpu
 def test_energy_conserved_to_second_order():
-    """No damping, no walls: the drift of the total energy over a fixed time
-    shrinks about fourfold when dt halves (velocity Verlet)."""
+    """No damping, no walls, bonded terms only: the largest deviation of the
+    total energy over a fixed time shrinks fourfold when dt halves (velocity
+    Verlet).  Contacts are left out because the penalty and the cut LJ force
+    have kinks, which lower the order; their potentials are checked against
+    the forces by finite differences above."""
     def drift(dt, steps):
         m = g.plain_network(seed=12, fibres=40, beads=20, box=(20.0, 20.0, 6.0), z_range=(1.0, 5.0),
-                            dt=dt)
+                            dt=dt, k_contact=0.0)
         m.vel = np.random.default_rng(3).normal(0.0, 0.2, m.vel.shape)
         m.vel_old = m.vel.copy()
         with sim(m) as s:
@@ -178,8 +178,8 @@ def test_energy_conserved_to_second_order():
         return dev / abs(e0)
     d1 = drift(0.002, 2000)
     d2 = drift(0.001, 4000)
-    assert d1 < 1e-2
-    assert d1 / d2 > 2.5, (d1, d2)
+    assert d1 < 1e-3
+    assert d1 / d2 > 3.5, (d1, d2)
 
 
 @pytest.mark.gpu
