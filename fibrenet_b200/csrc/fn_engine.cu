@@ -22,28 +22,14 @@
 #include <vector>
 
 #include "../../include/fibrenet.h"
+#include "fn_engine_internal.h"
 #include "fn_kernels.h"
 #include "fn_types.h"
 
+using fnh::DevBuf;
+using fnh::NetHost;
+
 namespace {
-
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-};
-
-/* Per-network host bookkeeping. */
-struct NetHost {
-    int bead_begin, bead_end;
-    int spring_begin, spring_end;
-    int angle_begin, angle_end;
-    long long cell_begin, cell_end;
-    int grid_update_freq;
-    double damping;
-    bool any_cut, any_hs; /* pair kinds present (listing radius) */
-    double rmax;          /* largest radius, as stored */
-};
 
 /* Largest listing radius squared of one network (kernel.cl:632-650): the
    cutoff for lj/st pairs, largest radius + largest skin for hs pairs. */
@@ -70,118 +56,12 @@ uint32_t spread10(uint32_t v) {
 
 }  // namespace
 
-struct fn_ctx {
-    fn_config cfg{};
-    cudaStream_t stream = nullptr;
-    std::string err;
-    bool uploaded = false;
 
-    int n_nets = 0;
-    std::vector<FnNet> nets_h;
-    std::vector<NetHost> info;
-    std::vector<FnPair> pairs_h;
-    long long nb = 0, ns = 0, na = 0, ncells = 0;
-    std::vector<int> perm;  // internal -> upload
-    std::vector<int> inv;   // upload -> internal
-    std::vector<double> mass_h, radius_h;
-    std::vector<float4> sp_par_h;  // upload order (springs are not renumbered)
-    std::vector<float2> an_par_h;
-    bool damp = false;
-    int grid_update_freq = 8;
-
-    DevBuf<double4> pos[2], img[2];
-    DevBuf<float4> vold, force, vel;
-    DevBuf<int4> binfo;
-    DevBuf<int2> sp_ends;
-    DevBuf<float4> sp_par;
-    DevBuf<signed char> sp_type, sp_status;
-    DevBuf<int4> an_b;
-    DevBuf<int2> an_s;
-    DevBuf<float2> an_par;
-    DevBuf<signed char> an_status;
-    DevBuf<int> sp_off, sp_ent, an_off, an_ent;
-    /* host copies of the incidence (internal numbering) for the tile lists */
-    std::vector<int> sp_off_h, sp_ent_h, an_off_h, an_ent_h;
-    std::vector<int4> an_b_h;
-    std::vector<int2> an_s_h;
-    /* per-tile bonded term lists of the tiled step kernel */
-    DevBuf<int> tile_sp_off, tile_sp, tile_an_off, tile_an, sp_slot, an_slot;
-    DevBuf<int2> tile_an_sslot;
-    int max_tile_sp = 0, max_tile_an = 0;
-    bool tiled = false;
-    /* chain form */
-    bool chain = false;
-    std::vector<int> sp_bead, an_bead; /* spring -> lower bead, angle -> centre bead */
-    std::vector<unsigned char> ch_flags_h;
-    DevBuf<float4> ch_sp;
-    DevBuf<float2> ch_an;
-    DevBuf<unsigned char> ch_flags, ch_status;
-    DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
-    DevBuf<int> scan_sums;
-    DevBuf<FnTile> tiles;
-    DevBuf<FnNet> nets;
-    DevBuf<FnPair> pairs;
-    DevBuf<unsigned long long> counters;
-    DevBuf<double> obs_partial, obs_out;
-    DevBuf<double> en_partial, en_out;
-    DevBuf<double> series; /* rows of fn_step_series */
-    int list_stride = 0;
-    int cur = 0;
-    int block = 128;
-    int ntiles = 0;
-    long long device_bytes = 0;
-    long long steps_done = 0, rebuilds_done = 0;
-
-    /* captured step segments: (parity, length, ends the call) -> graph */
-    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
-    long long graph_launches = 0;
-
-    bool timing = false;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_step, ev_rebuild;
-    size_t ev_next = 0;
-};
-
-namespace {
+namespace fnh {
 
 int fail(fn_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
-}
-
-#define CK(call)                                                                          \
-    do {                                                                                  \
-        cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(c, e_ == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA,    \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));              \
-    } while (0)
-
-template <class T>
-cudaError_t dalloc(fn_ctx* c, DevBuf<T>& b, size_t n) {
-    if (b.p) {
-        cudaFree(b.p);
-        c->device_bytes -= (long long)(b.n * sizeof(T));
-        b.p = nullptr;
-        b.n = 0;
-    }
-    size_t bytes = sizeof(T) * (n ? n : 1);
-    cudaError_t e = cudaMalloc((void**)&b.p, bytes);
-    if (e == cudaSuccess) {
-        b.n = n ? n : 1;
-        c->device_bytes += (long long)bytes;
-    }
-    return e;
-}
-
-template <class T>
-void dfree(fn_ctx* c, DevBuf<T>& b) {
-    if (b.p) {
-        cudaFree(b.p);
-        c->device_bytes -= (long long)(b.n * sizeof(T));
-    }
-    b.p = nullptr;
-    b.n = 0;
 }
 
 template <class T>
@@ -245,6 +125,7 @@ void free_all(fn_ctx* c) {
     dfree(c, c->en_partial);
     dfree(c, c->en_out);
     dfree(c, c->series);
+    adjoint_free(c);
 }
 
 /* Kernel constants of one network (SimulationManager.cpp:647-671, 684-720,
@@ -751,7 +632,9 @@ int check_ready(fn_ctx* c) {
     return FN_OK;
 }
 
-}  // namespace
+}  // namespace fnh
+
+using namespace fnh;
 
 /* ======================================================================== */
 
@@ -800,6 +683,7 @@ FN_API void fn_destroy(fn_ctx* c) {
 FN_API const char* fn_last_error(const fn_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
+    if (c) c->state_version++;
     if (!c || n_networks <= 0 || !nets) return fail(c, FN_ERR_ARG, "fn_upload: bad arguments");
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
@@ -1087,6 +971,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
 }
 
 FN_API int fn_step(fn_ctx* c, int nsteps) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     if (nsteps <= 0) return fail(c, FN_ERR_ARG, "RunSimulationLoop: loop size should be a positive number");
@@ -1117,6 +1002,7 @@ FN_API int fn_rebuild_contacts(fn_ctx* c) {
 }
 
 FN_API int fn_reset_energy(fn_ctx* c) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1168,6 +1054,7 @@ FN_API int fn_download(fn_ctx* c, int field, double* host) {
 }
 
 FN_API int fn_set_beads(fn_ctx* c, int field, const double* host) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     if (!host) return fail(c, FN_ERR_ARG, "fn_set_beads: null host pointer");
@@ -1202,6 +1089,7 @@ FN_API int fn_set_beads(fn_ctx* c, int field, const double* host) {
 }
 
 FN_API int fn_set_mass(fn_ctx* c, const double* mass) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     if (!mass) return fail(c, FN_ERR_ARG, "fn_set_mass: null pointer");
@@ -1222,6 +1110,7 @@ FN_API int fn_set_mass(fn_ctx* c, const double* mass) {
 }
 
 FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     if (!skin) return fail(c, FN_ERR_ARG, "fn_set_skin: null pointer");
@@ -1244,6 +1133,7 @@ FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
 
 FN_API int fn_set_springs(fn_ctx* c, const double* rest, const double* k, const double* c1,
                           const double* c2) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1266,6 +1156,7 @@ FN_API int fn_set_springs(fn_ctx* c, const double* rest, const double* k, const 
 }
 
 FN_API int fn_set_angles(fn_ctx* c, const double* theta0, const double* k) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1312,6 +1203,7 @@ FN_API int fn_download_status(fn_ctx* c, int* spring_status, int* angle_status) 
 }
 
 FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_status) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1674,6 +1566,7 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
 /* Forces alone at the current positions (zeroed, no base term), for the
    one-step parity checks: terms bit 0 springs, 1 angles, 2 contacts. */
 FN_API int fn_forces_only(fn_ctx* c, int terms) {
+    if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));

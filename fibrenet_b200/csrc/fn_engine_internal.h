@@ -1,0 +1,174 @@
+/*
+ * fn_engine_internal.h -- the context behind the C ABI, shared by the engine
+ * (fn_engine.cu) and the adjoint (fn_adjoint.cu).  Not a public header.
+ */
+#ifndef FIBRENET_ENGINE_INTERNAL_H
+#define FIBRENET_ENGINE_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <tuple>
+#include <utility>
+#include <vector>
+
+#include "../../include/fibrenet.h"
+#include "fn_kernels.h"
+#include "fn_types.h"
+
+namespace fnh {
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+};
+
+/* Per-network host bookkeeping. */
+struct NetHost {
+    int bead_begin, bead_end;
+    int spring_begin, spring_end;
+    int angle_begin, angle_end;
+    long long cell_begin, cell_end;
+    int grid_update_freq;
+    double damping;
+    bool any_cut, any_hs; /* pair kinds present (listing radius) */
+    double rmax;          /* largest radius, as stored */
+};
+
+struct AdjointState; /* fn_adjoint.cu */
+
+}  // namespace fnh
+
+struct fn_ctx {
+    using NetHost = fnh::NetHost;
+    template <class T>
+    using DevBuf = fnh::DevBuf<T>;
+
+    fn_config cfg{};
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool uploaded = false;
+
+    int n_nets = 0;
+    std::vector<FnNet> nets_h;
+    std::vector<NetHost> info;
+    std::vector<FnPair> pairs_h;
+    long long nb = 0, ns = 0, na = 0, ncells = 0;
+    std::vector<int> perm;  // internal -> upload
+    std::vector<int> inv;   // upload -> internal
+    std::vector<double> mass_h, radius_h;
+    std::vector<float4> sp_par_h;  // upload order (springs are not renumbered)
+    std::vector<float2> an_par_h;
+    bool damp = false;
+    int grid_update_freq = 8;
+
+    DevBuf<double4> pos[2], img[2];
+    DevBuf<float4> vold, force, vel;
+    DevBuf<int4> binfo;
+    DevBuf<int2> sp_ends;
+    DevBuf<float4> sp_par;
+    DevBuf<signed char> sp_type, sp_status;
+    DevBuf<int4> an_b;
+    DevBuf<int2> an_s;
+    DevBuf<float2> an_par;
+    DevBuf<signed char> an_status;
+    DevBuf<int> sp_off, sp_ent, an_off, an_ent;
+    /* host copies of the incidence (internal numbering) for the tile lists */
+    std::vector<int> sp_off_h, sp_ent_h, an_off_h, an_ent_h;
+    std::vector<int4> an_b_h;
+    std::vector<int2> an_s_h;
+    /* per-tile bonded term lists of the tiled step kernel */
+    DevBuf<int> tile_sp_off, tile_sp, tile_an_off, tile_an, sp_slot, an_slot;
+    DevBuf<int2> tile_an_sslot;
+    int max_tile_sp = 0, max_tile_an = 0;
+    bool tiled = false;
+    /* chain form */
+    bool chain = false;
+    std::vector<int> sp_bead, an_bead; /* spring -> lower bead, angle -> centre bead */
+    std::vector<unsigned char> ch_flags_h;
+    DevBuf<float4> ch_sp;
+    DevBuf<float2> ch_an;
+    DevBuf<unsigned char> ch_flags, ch_status;
+    DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
+    DevBuf<int> scan_sums;
+    DevBuf<FnTile> tiles;
+    DevBuf<FnNet> nets;
+    DevBuf<FnPair> pairs;
+    DevBuf<unsigned long long> counters;
+    DevBuf<double> obs_partial, obs_out;
+    DevBuf<double> en_partial, en_out;
+    DevBuf<double> series; /* rows of fn_step_series */
+    int list_stride = 0;
+    int cur = 0;
+    int block = 128;
+    int ntiles = 0;
+    long long device_bytes = 0;
+    long long steps_done = 0, rebuilds_done = 0;
+
+    /* captured step segments: (parity, length, ends the call) -> graph */
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;
+    long long graph_launches = 0;
+
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_step, ev_rebuild;
+    size_t ev_next = 0;
+
+    /* bumped by every call that changes the state or the parameters */
+    long long state_version = 0;
+    /* differentiation state (fn_adjoint_*), null until first used */
+    fnh::AdjointState* adj = nullptr;
+};
+
+namespace fnh {
+
+int fail(fn_ctx* c, int code, const std::string& msg);
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return ::fnh::fail(c, e_ == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA, \
+                               std::string(#call) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(fn_ctx* c, DevBuf<T>& b, size_t n) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->device_bytes -= (long long)(b.n * sizeof(T));
+        b.p = nullptr;
+        b.n = 0;
+    }
+    size_t bytes = sizeof(T) * (n ? n : 1);
+    cudaError_t e = cudaMalloc((void**)&b.p, bytes);
+    if (e == cudaSuccess) {
+        b.n = n ? n : 1;
+        c->device_bytes += (long long)bytes;
+    }
+    return e;
+}
+
+template <class T>
+void dfree(fn_ctx* c, DevBuf<T>& b) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->device_bytes -= (long long)(b.n * sizeof(T));
+    }
+    b.p = nullptr;
+    b.n = 0;
+}
+
+int check_ready(fn_ctx* c);
+fn::StepArgs step_args(fn_ctx* c, bool pingpong);
+fn::RebuildArgs rebuild_args(fn_ctx* c);
+void drop_graphs(fn_ctx* c);
+
+/* adjoint state teardown (fn_adjoint.cu), called by free_all */
+void adjoint_free(fn_ctx* c);
+
+}  // namespace fnh
+
+#endif

@@ -24,19 +24,12 @@
 #include <stdint.h>
 
 #include "fn_detmath.h"
+#include "fn_device.cuh"
 #include "fn_kernels.h"
 #include "fn_types.h"
 
 namespace fn {
 
-__device__ __forceinline__ float w_radius(double w) { return __int_as_float(__double2loint(w)); }
-__device__ __forceinline__ int w_type(double w) { return __double2hiint(w); }
-
-/* GETADRESS, kernel.cl:9 */
-__device__ __forceinline__ int getadress(int t1, int t2, int size) {
-    return (t1 < t2) ? ((size * t1) + t2 - ((t1 * (t1 + 1)) / 2))
-                     : ((size * t2) + t1 - ((t2 * (t2 + 1)) / 2));
-}
 
 __device__ __forceinline__ int spring_pts(double ax, double ay, double az, double bx, double by,
                                           double bz, float4 par, int type, double& fx, double& fy,
@@ -141,19 +134,6 @@ __device__ __forceinline__ void angle_eval(const StepArgs& A, int4 b, float2 par
     const double4 t3 = A.img_in[b.z];
     angle_pts(t1.x, t1.y, t1.z, t2.x, t2.y, t2.z, t3.x, t3.y, t3.z, par, pax, pay, paz, pcx, pcy,
               pcz);
-}
-
-/* Minimum image on the axes of mask (kernel.cl:598-627, 844-870). */
-__device__ __forceinline__ double min_image(const FnNet& N, double& rx, double& ry, double& rz,
-                                            double length, int mask) {
-    const double maxDim = N.half_box_sq;
-    if (length > maxDim) {
-        if ((mask & 1) && rx * rx > maxDim) rx = rx > 0.0 ? rx - N.box[0] : rx + N.box[0];
-        if ((mask & 2) && ry * ry > maxDim) ry = ry > 0.0 ? ry - N.box[1] : ry + N.box[1];
-        if ((mask & 4) && rz * rz > maxDim) rz = rz > 0.0 ? rz - N.box[2] : rz + N.box[2];
-        length = rx * rx + ry * ry + rz * rz;
-    }
-    return length;
 }
 
 /* One contact-list entry (kernel.cl:835-999): force on bead i. */

@@ -102,6 +102,9 @@ SIGNATURES = {
     "fn_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FnStats)]),
     "fn_observe_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "fn_energy_eval": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FnEnergy)]),
+    "fn_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _D]),
+    "fn_adjoint_backward": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D, _D]),
+    "fn_adjoint_release": (C.c_int, [C.c_void_p]),
     "fn_step_series": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _D]),
     "fn_get_cells": (C.c_int, [C.c_void_p, _I, _I, C.c_longlong]),
     "fn_get_lists": (C.c_int, [C.c_void_p, _I, _I, C.c_int]),
@@ -327,6 +330,32 @@ class Simulation:
         self._check(self.lib.fn_step_series(self.h, nsteps, every, net, reaction_type, int(energy),
                                             out.ctypes.data_as(_D)))
         return out
+
+    # --- differentiation
+    def adjoint_forward(self, nsamples: int, every: int, checkpoint_every: int,
+                        reaction_type: int) -> np.ndarray:
+        """nsamples step(every) calls with checkpoints; returns the reaction of
+        every network after each call, [nsamples, n_networks, 3]."""
+        out = np.zeros((nsamples, len(self.models), 3), np.float64)
+        self._check(self.lib.fn_adjoint_forward(self.h, nsamples, every, checkpoint_every,
+                                                reaction_type, out.ctypes.data_as(_D)))
+        return out
+
+    def adjoint_backward(self, dloss_dreaction) -> dict:
+        """Gradients for dL/d reaction ([nsamples, n_networks, 3]): spring_k,
+        spring_rest (per spring), angle_k (per angle), pos0 and vel0 (per
+        bead, [n, 3]), all in upload order."""
+        g = np.ascontiguousarray(dloss_dreaction, np.float64)
+        out = {"spring_k": np.zeros(self.ns), "spring_rest": np.zeros(self.ns),
+               "angle_k": np.zeros(self.na), "pos0": np.zeros((self.nb, 3)),
+               "vel0": np.zeros((self.nb, 3))}
+        self._check(self.lib.fn_adjoint_backward(
+            self.h, g.ctypes.data_as(_D), *[out[k].ctypes.data_as(_D) for k in
+                                            ("spring_k", "spring_rest", "angle_k", "pos0", "vel0")]))
+        return out
+
+    def adjoint_release(self) -> None:
+        self._check(self.lib.fn_adjoint_release(self.h))
 
     def stats(self) -> dict:
         s = FnStats()

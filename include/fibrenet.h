@@ -225,6 +225,34 @@ FN_API int fn_observe(fn_ctx* ctx, int net, int reaction_type, fn_observables* o
 
 FN_API int fn_get_stats(fn_ctx* ctx, fn_stats* out);
 
+/* ---- differentiation (no counterpart in the reference) ----------------
+   Gradients of a loss on the recorded reaction force with respect to every
+   spring stiffness and rest length, every angle stiffness and the initial
+   positions and velocities, by the discrete adjoint of the step loop.
+
+   fn_adjoint_forward runs nsamples fn_step(every) calls from the current
+   state, records after each the reaction of every network (the force summed
+   over its beads of type reaction_type) into reaction[nsamples][n_networks][3]
+   (may be null), and keeps a device checkpoint every checkpoint_every steps
+   (a multiple of every dividing nsamples * every).  Needs damping 0.
+
+   fn_adjoint_backward takes dL/d reaction in the same layout and writes the
+   gradients (any output may be null): per spring and per angle in upload
+   order, per bead [n_beads][3] in upload order for the positions and
+   velocities the forward pass started from.  Contact sets, the contact list
+   of each rebuild interval and HR_FL break events are those of the forward
+   pass; segments are recomputed from their checkpoints (checked bit for bit
+   against the next checkpoint).  It leaves the state where the forward pass
+   ended; any state change in between makes it fail with FN_ERR_STATE.
+   Device memory: 128 B per bead per checkpoint step of replay, 112 B per
+   bead per checkpoint.  fn_adjoint_release frees it. */
+FN_API int fn_adjoint_forward(fn_ctx* ctx, int nsamples, int every, int checkpoint_every,
+                              int reaction_type, double* reaction);
+FN_API int fn_adjoint_backward(fn_ctx* ctx, const double* dloss_dreaction, double* grad_spring_k,
+                               double* grad_spring_rest, double* grad_angle_k, double* grad_pos0,
+                               double* grad_vel0);
+FN_API int fn_adjoint_release(fn_ctx* ctx);
+
 /* Energy and virial of network `net` at the current state (after fn_step the
    state holds the positions its last forces were evaluated at). */
 FN_API int fn_energy_eval(fn_ctx* ctx, int net, fn_energy* out);
