@@ -47,14 +47,19 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
-    p.add_argument("--workload", choices=["tensile", "dense", "ensemble"], default="tensile",
+    p.add_argument("--workload", choices=["tensile", "dense", "ensemble", "adjoint"], default="tensile",
                    help="tensile: the 1M-bead network (default, the headline); dense: the 4M-bead "
                         "periodic 3D mat with penalty + soft-repulsion contacts; ensemble: 256 "
-                        "independent networks batched in one context vs run one by one")
-    p.add_argument("--networks", type=int, default=256)
+                        "independent networks batched in one context vs run one by one; adjoint: "
+                        "64 networks, reaction-curve loss, forward + backward sweep vs forward")
+    p.add_argument("--networks", type=int, default=None)
+    p.add_argument("--adam-iters", type=int, default=0,
+                   help="adjoint workload: stiffness-recovery iterations after the timing")
     a = p.parse_args()
     if a.fibres is None:
         a.fibres = 40000 if a.workload == "dense" else 20000
+    if a.networks is None:
+        a.networks = 64 if a.workload == "adjoint" else 256
     return a
 
 
@@ -497,12 +502,137 @@ def run_ensemble(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args):
+    """Stiffness fitting: 64 tensile networks in one context, loss = squared
+    error of the x reaction curve (sampled every 20 steps) against a target
+    run with lognormal(0, 0.2)-perturbed stiffnesses.  Times the plain
+    forward, the recorded forward (checkpoints every 100 steps) and the
+    backward sweep (segment replay + adjoint), each with CUDA events."""
+    import numpy as np
+    import torch
+
+    from fibrenet_b200 import generate as g
+    from fibrenet_b200.fitting import ReactionCurve
+    from fibrenet_b200.ranks import partition_networks
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    every, ckpt = 20, 100
+    steps = max(ckpt, (args.steps // ckpt) * ckpt)
+    nsamples = steps // every
+    all_ms = g.fitting_networks(seed=4, n_networks=args.networks)
+    mine = partition_networks([m.n_beads for m in all_ms], world)[rank]
+    ms = [all_ms[i] for i in mine]
+    nb = sum(m.n_beads for m in ms)
+    CR = 2
+    target_ms = g.perturbed_stiffness(ms, seed=5)
+    tgt = ReactionCurve(target_ms, nsamples, every, ckpt, CR, device=local, use_graphs=True)
+    target = tgt.run(tgt.params["spring_k"], tgt.params["spring_rest"], tgt.params["angle_k"])
+    tgt.close()
+    curve = ReactionCurve(ms, nsamples, every, ckpt, CR, device=local, use_graphs=True)
+    k0, r0, a0 = curve.params["spring_k"], curve.params["spring_rest"], curve.params["angle_k"]
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        e0, e1 = ev(), ev()
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        curve.sim.sync()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    # warm-up: graphs, replay buffers
+    R = curve.run(k0, r0, a0)
+    curve.sim.adjoint_backward(np.zeros_like(R))
+
+    def plain():
+        curve._load(k0, r0, a0, None)
+        curve.sim.sync()
+        e0, e1 = ev(), ev()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(nsamples):
+            curve.sim.step(every)
+            curve.sim.observe_noalloc(obs.data_ptr(), 0, CR)
+        curve.sim.sync()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    obs = torch.zeros(5, dtype=torch.float64, device=f"cuda:{local}")
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_plain = plain()
+    curve._load(k0, r0, a0, None)
+    R, t_fwd = timed(lambda: curve.sim.adjoint_forward(nsamples, every, ckpt, CR))
+    dR = np.zeros_like(R)
+    dR[..., 0] = 2.0 * (R[..., 0] - target[..., 0])
+    grads, t_bwd = timed(lambda: curve.sim.adjoint_backward(dR))
+    clk = clocks.stop()
+    loss0 = float(((R[..., 0] - target[..., 0]) ** 2).sum())
+    fit = None
+    if args.adam_iters > 0:
+        logk = torch.tensor(np.log(k0), requires_grad=True)
+        opt = torch.optim.Adam([logk], lr=0.02)
+        rest_t, ka_t = torch.tensor(r0), torch.tensor(a0)
+        tgt_t = torch.tensor(target[..., 0])
+        hist = []
+        for _ in range(args.adam_iters):
+            opt.zero_grad()
+            Rt = curve(torch.exp(logk), rest_t, ka_t)
+            loss = ((Rt[..., 0] - tgt_t) ** 2).sum()
+            loss.backward()
+            opt.step()
+            hist.append(float(loss.detach()))
+        true_k = np.concatenate([np.asarray(t.s_k, np.float64) for t in target_ms])
+        k_fit = np.exp(logk.detach().numpy())
+        fit = {"iterations": args.adam_iters, "loss_first": hist[0], "loss_last": hist[-1],
+               "median_rel_err_k_start": float(np.median(np.abs(k0 / true_k - 1))),
+               "median_rel_err_k_fit": float(np.median(np.abs(k_fit / true_k - 1)))}
+    curve.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": "adjoint/forward time (64-network tensile fit, 1 B200)",
+            "value": t_bwd / t_plain, "unit": "ratio", "n_gpus": world, "steps": steps, "warmup": 1,
+            "ms_per_step": t_bwd / steps, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 forces / f32 state / f64 gradient sums",
+            "data": "synthetic (seeded generator; target from lognormal(0, 0.2) stiffness factors)",
+            "config": {"workload": f"fit_{len(all_ms)}", "networks": len(all_ms), "beads": nb,
+                       "every": every, "checkpoint_every": ckpt, "loss": "sum (R_x - R*_x)^2",
+                       "params": {"spring_k": len(k0), "spring_rest": len(r0), "angle_k": len(a0),
+                                  "pos0": 3 * nb}},
+            "forward_ms": t_plain, "recorded_forward_ms": t_fwd, "backward_ms": t_bwd,
+            "forward_bead_steps_per_s": nb * steps / (t_plain / 1e3),
+            "backward_over_recorded_forward": t_bwd / t_fwd, "loss": loss0,
+            "grad_norm": {k: float(np.linalg.norm(v)) for k, v in grads.items()},
+            "fit": fit, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
     elif args.workload == "ensemble":
         run_ensemble(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

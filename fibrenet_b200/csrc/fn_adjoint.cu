@@ -99,6 +99,63 @@ __device__ void angle_dual(const double* t1, const double* t2, const double* t3,
     for (int a = 0; a < 3; ++a) pc[a] = pc[a] * sc;
 }
 
+__device__ __forceinline__ Dual dsin(Dual a) { return {sin(a.v), cos(a.v) * a.d}; }
+
+/* The same angle force for a rest angle of pi in its regular form
+     pa = 2k G (w - cos(theta) u) / |ba|,  pc = 2k G (u - cos(theta) w) / |bc|,
+     G = (theta - pi) / sin(theta) = -phi / sin(phi),  phi = pi - theta,
+   with u, w the unit arms (at unit stiffness).  It equals kernel.cl's cross-
+   product form for theta0 = pi.  A rest angle stored as the FP32 rounding
+   of pi adds a term of constant size 2k (theta0 - pi) / |ba| whose direction
+   turns with the bend, so its Jacobian grows like (theta0 - pi) / phi and is
+   unbounded for the straight fibres the tensile networks start from; the
+   adjoint differentiates the regular form (the dropped term is below 1.8e-6
+   k / |ba| in force).  phi^2 comes from |u + w|^2 = 4 sin^2(phi / 2), which
+   keeps full precision near straight.  Exactly straight triples (zero cross
+   product, where the step applies no force) get no tangent. */
+__device__ void angle_dual_straight(const double* t1, const double* t2, const double* t3,
+                                    const float* w1, const float* w2, const float* w3, Dual pa[3],
+                                    Dual pc[3]) {
+    Dual ba[3], bc[3];
+    for (int a = 0; a < 3; ++a) {
+        ba[a] = {t1[a] - t2[a], (double)w1[a] - (double)w2[a]};
+        bc[a] = {t3[a] - t2[a], (double)w3[a] - (double)w2[a]};
+    }
+    const double cx = ba[1].v * bc[2].v - ba[2].v * bc[1].v;
+    const double cy = ba[2].v * bc[0].v - ba[0].v * bc[2].v;
+    const double cz = ba[0].v * bc[1].v - ba[1].v * bc[0].v;
+    if (cx == 0.0 && cy == 0.0 && cz == 0.0) {
+        for (int a = 0; a < 3; ++a) pa[a] = pc[a] = dl(0.0);
+        return;
+    }
+    const Dual l_ba = dsqrt(ba[0] * ba[0] + ba[1] * ba[1] + ba[2] * ba[2]);
+    const Dual l_bc = dsqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]);
+    Dual u[3], w[3];
+    for (int a = 0; a < 3; ++a) {
+        u[a] = ba[a] / l_ba;
+        w[a] = bc[a] / l_bc;
+    }
+    const Dual c = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
+    const Dual q = (u[0] + w[0]) * (u[0] + w[0]) + (u[1] + w[1]) * (u[1] + w[1]) +
+                   (u[2] + w[2]) * (u[2] + w[2]);
+    Dual G;
+    if (q.v < 1e-2) {
+        /* phi^2 = q + q^2/12 + q^3/90;  -G = 1 + p/6 + 7p^2/360 + 31p^3/15120 */
+        const Dual p = q + q * q * (1.0 / 12.0) + q * q * q * (1.0 / 90.0);
+        G = (dl(1.0) + p * (1.0 / 6.0) + p * p * (7.0 / 360.0) + p * p * p * (31.0 / 15120.0)) * -1.0;
+    } else {
+        const Dual sq = dsqrt(q);
+        const double h = sq.v * 0.5;
+        const Dual phi = {2.0 * asin(h), h < 1.0 ? sq.d / sqrt(1.0 - h * h) : 0.0};
+        G = (phi / dsin(phi)) * -1.0;
+    }
+    const Dual sa = G * 2.0 / l_ba, sc = G * 2.0 / l_bc;
+    for (int a = 0; a < 3; ++a) {
+        pa[a] = (w[a] - c * u[a]) * sa;
+        pc[a] = (u[a] - c * w[a]) * sc;
+    }
+}
+
 /* Tangent of a central pair force f(r) r_hat along dr: (f/r)(dr - r_hat
    (r_hat.dr)) + f'(r) r_hat (r_hat.dr). */
 __device__ __forceinline__ void central_tangent(double rx, double ry, double rz, double r, double f,
@@ -247,7 +304,10 @@ __global__ void __launch_bounds__(256) k_adj_bonds(const AdjArgs A) {
         const float f1[3] = {w1.x, w1.y, w1.z}, f2[3] = {w2.x, w2.y, w2.z}, f3[3] = {w3.x, w3.y, w3.z};
         const float2 par = A.an_par[q];
         Dual pa[3], pc[3];
-        angle_dual(t1, t2, t3, f1, f2, f3, (double)par.x, pa, pc);
+        if (fabs((double)par.x - 3.14159265358979323846) < 1e-6)
+            angle_dual_straight(t1, t2, t3, f1, f2, f3, pa, pc);
+        else
+            angle_dual(t1, t2, t3, f1, f2, f3, (double)par.x, pa, pc);
         const double k = par.y;
         o1 = make_float4((float)(k * pa[0].d), (float)(k * pa[1].d), (float)(k * pa[2].d), 0.f);
         o3 = make_float4((float)(k * pc[0].d), (float)(k * pc[1].d), (float)(k * pc[2].d), 0.f);
@@ -356,15 +416,20 @@ __global__ void k_adj_start(const AdjArgs A) {
     A.V[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-/* Reaction of every network at once (one block per network): the sum of
-   the force on beads of the reaction type, fixed-order FP64 reduction. */
-__global__ void __launch_bounds__(256) k_reaction_all(const FnNet* nets, const double4* pos,
-                                                      const float4* force, int reaction_type,
-                                                      double* out) {
+/* Reaction of every network at once: blocks (chunk, network) sum the force
+   on beads of the reaction type over 2048-bead chunks, then one thread per
+   network adds its chunks in order (fixed-order FP64 reduction). */
+constexpr int kReactionChunk = 2048;
+
+__global__ void __launch_bounds__(256) k_reaction_partial(const FnNet* nets, const double4* pos,
+                                                          const float4* force, int reaction_type,
+                                                          double* partial) {
     __shared__ double sx[256], sy[256], sz[256];
-    const FnNet& N = nets[blockIdx.x];
+    const FnNet& N = nets[blockIdx.y];
+    const int begin = N.bead_begin + blockIdx.x * kReactionChunk;
+    const int end = min(N.bead_end, begin + kReactionChunk);
     double x = 0.0, y = 0.0, z = 0.0;
-    for (int i = N.bead_begin + threadIdx.x; i < N.bead_end; i += blockDim.x) {
+    for (int i = begin + threadIdx.x; i < end; i += blockDim.x) {
         if (w_type(pos[i].w) == reaction_type) {
             const float4 f = force[i];
             x += (double)f.x;
@@ -385,10 +450,41 @@ __global__ void __launch_bounds__(256) k_reaction_all(const FnNet* nets, const d
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        out[3 * blockIdx.x] = sx[0];
-        out[3 * blockIdx.x + 1] = sy[0];
-        out[3 * blockIdx.x + 2] = sz[0];
+        double* o = partial + 3 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x);
+        o[0] = sx[0];
+        o[1] = sy[0];
+        o[2] = sz[0];
     }
+}
+
+__global__ void k_reaction_final(const double* partial, int nchunks, int n_nets, double* out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= n_nets) return;
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (int k = 0; k < nchunks; ++k) {
+        const double* p = partial + 3 * ((size_t)n * nchunks + k);
+        x += p[0];
+        y += p[1];
+        z += p[2];
+    }
+    out[3 * n] = x;
+    out[3 * n + 1] = y;
+    out[3 * n + 2] = z;
+}
+
+/* Copies the first max(count) columns of a column-major contact list. */
+__global__ void k_list_max(const int* count, int n, int cap, int* kmax) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicMax(kmax, min(count[i], cap));
+}
+
+__global__ void k_list_copy(const int* count, const int* list, int n, int stride, const int* kmax,
+                            int* count_out, int* list_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    count_out[i] = count[i];
+    const int km = *kmax;
+    for (int k = 0; k < km; ++k) list_out[(size_t)k * stride + i] = list[(size_t)k * stride + i];
 }
 
 /* Counts beads whose positions differ bit-wise between two buffers. */
@@ -421,6 +517,9 @@ struct AdjointState {
     /* replay */
     DevBuf<double4> rec_pos, rec_img;
     DevBuf<unsigned char> rec_st;
+    DevBuf<int> rec_count, rec_list, kmax; /* the contact list of each rebuild in the segment */
+    DevBuf<double> react_partial;
+    int nchunks = 1;
     /* adjoint */
     DevBuf<float4> X, V, fbar[2], sp_tan, an_tan;
     DevBuf<double2> g_spring;
@@ -443,6 +542,10 @@ void adjoint_free(fn_ctx* c) {
     dfree(c, S->rec_pos);
     dfree(c, S->rec_img);
     dfree(c, S->rec_st);
+    dfree(c, S->rec_count);
+    dfree(c, S->rec_list);
+    dfree(c, S->kmax);
+    dfree(c, S->react_partial);
     dfree(c, S->X);
     dfree(c, S->V);
     dfree(c, S->fbar[0]);
@@ -458,6 +561,14 @@ void adjoint_free(fn_ctx* c) {
 }
 
 namespace {
+
+/* Grows a buffer to at least n elements (buffers are kept between calls so
+   a fitting loop allocates once). */
+template <class T>
+cudaError_t ensure(fn_ctx* c, DevBuf<T>& b, size_t n) {
+    if (b.p && b.n >= n) return cudaSuccess;
+    return dalloc(c, b, n);
+}
 
 size_t status_bytes(fn_ctx* c) { return c->chain ? (size_t)c->nb : (size_t)(c->ns + c->na); }
 
@@ -522,6 +633,20 @@ int rebuild_from(fn_ctx* c, const double4* pos) {
     return FN_OK;
 }
 
+/* Records the current contact list (its used columns only) in slot. */
+int save_list(fn_ctx* c, int slot) {
+    AdjointState* S = c->adj;
+    const size_t nb = (size_t)c->nb, stride = (size_t)c->list_stride;
+    CK(cudaMemsetAsync(S->kmax.p, 0, sizeof(int), c->stream));
+    const int nblk = (int)((nb + 255) / 256);
+    fn::k_list_max<<<nblk, 256, 0, c->stream>>>(c->list_count.p, (int)nb, c->cfg.list_capacity, S->kmax.p);
+    fn::k_list_copy<<<nblk, 256, 0, c->stream>>>(c->list_count.p, c->list.p, (int)nb, (int)stride, S->kmax.p,
+                                                  S->rec_count.p + (size_t)slot * nb,
+                                                  S->rec_list.p + (size_t)slot * stride * c->cfg.list_capacity);
+    CK(cudaGetLastError());
+    return FN_OK;
+}
+
 /* Evaluation index (within a segment) where the contact list used by each
    evaluation was built: the schedule of fn_step (a call opens with a drift,
    then rebuild-led runs of grid_update_freq steps). */
@@ -544,6 +669,7 @@ int replay_segment(fn_ctx* c, int q) {
     const size_t nb = (size_t)c->nb;
     int r = load_checkpoint(c, q);
     if (r) return r;
+    int slot = 0;
     auto P = [&](int j) { return S->rec_pos.p + (size_t)j * nb; };
     auto I = [&](int j) { return S->rec_img.p + (size_t)j * nb; };
     for (int call0 = 0; call0 < K; call0 += every) {
@@ -559,6 +685,8 @@ int replay_segment(fn_ctx* c, int q) {
             const int len = std::min(gu, every - done);
             const bool tail = done + len == every;
             r = rebuild_from(c, P(call0 + done));
+            if (r) return r;
+            r = save_list(c, slot++);
             if (r) return r;
             for (int k = 0; k < len; ++k) {
                 const int j = call0 + done + k;
@@ -653,9 +781,9 @@ FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint
     const long long total = (long long)nsamples * every;
     if (total % checkpoint_every != 0)
         return fail(c, FN_ERR_ARG, "fn_adjoint_forward: nsamples * every must be a multiple of checkpoint_every");
-    adjoint_free(c);
-    c->adj = new AdjointState();
+    if (!c->adj) c->adj = new AdjointState();
     AdjointState* S = c->adj;
+    S->version = -1;
     S->every = every;
     S->nsamples = nsamples;
     S->ckpt_every = checkpoint_every;
@@ -663,15 +791,19 @@ FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint
     S->nckpt = (int)(total / checkpoint_every);
     S->st_bytes = status_bytes(c);
     const size_t nb = (size_t)c->nb, slots = (size_t)S->nckpt + 1;
-    CK(dalloc(c, S->ck_pos, slots * nb));
-    CK(dalloc(c, S->ck_img, slots * nb));
-    CK(dalloc(c, S->ck_vold, slots * nb));
-    CK(dalloc(c, S->ck_force, slots * nb));
-    CK(dalloc(c, S->ck_vel, slots * nb));
-    CK(dalloc(c, S->ck_st, slots * S->st_bytes));
-    CK(dalloc(c, S->saved_count, nb));
-    CK(dalloc(c, S->saved_list, (size_t)c->list_stride * c->cfg.list_capacity));
-    CK(dalloc(c, S->reaction, (size_t)nsamples * c->n_nets * 3));
+    CK(ensure(c, S->ck_pos, slots * nb));
+    CK(ensure(c, S->ck_img, slots * nb));
+    CK(ensure(c, S->ck_vold, slots * nb));
+    CK(ensure(c, S->ck_force, slots * nb));
+    CK(ensure(c, S->ck_vel, slots * nb));
+    CK(ensure(c, S->ck_st, slots * S->st_bytes));
+    CK(ensure(c, S->saved_count, nb));
+    CK(ensure(c, S->saved_list, (size_t)c->list_stride * c->cfg.list_capacity));
+    CK(ensure(c, S->reaction, (size_t)nsamples * c->n_nets * 3));
+    int maxb = 1;
+    for (int k = 0; k < c->n_nets; ++k) maxb = std::max(maxb, c->info[k].bead_end - c->info[k].bead_begin);
+    S->nchunks = (maxb + fn::kReactionChunk - 1) / fn::kReactionChunk;
+    CK(ensure(c, S->react_partial, (size_t)3 * S->nchunks * c->n_nets));
     for (int s = 0; s < nsamples; ++s) {
         if (((long long)s * every) % checkpoint_every == 0) {
             r = save_checkpoint(c, (int)(((long long)s * every) / checkpoint_every));
@@ -679,8 +811,10 @@ FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint
         }
         r = fn_step(c, every);
         if (r) return r;
-        fn::k_reaction_all<<<c->n_nets, 256, 0, c->stream>>>(c->nets.p, c->pos[c->cur].p, c->force.p, reaction_type,
-                                                             S->reaction.p + (size_t)s * c->n_nets * 3);
+        fn::k_reaction_partial<<<dim3(S->nchunks, c->n_nets), 256, 0, c->stream>>>(
+            c->nets.p, c->pos[c->cur].p, c->force.p, reaction_type, S->react_partial.p);
+        fn::k_reaction_final<<<(c->n_nets + 127) / 128, 128, 0, c->stream>>>(
+            S->react_partial.p, S->nchunks, c->n_nets, S->reaction.p + (size_t)s * c->n_nets * 3);
         CK(cudaGetLastError());
     }
     r = save_checkpoint(c, S->nckpt);
@@ -708,20 +842,30 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
     CK(cudaSetDevice(c->cfg.device));
     const size_t nb = (size_t)c->nb;
     const int K = S->ckpt_every;
-    CK(dalloc(c, S->rec_pos, (size_t)K * nb));
-    CK(dalloc(c, S->rec_img, (size_t)K * nb));
-    CK(dalloc(c, S->rec_st, (size_t)K * S->st_bytes));
-    CK(dalloc(c, S->X, nb));
-    CK(dalloc(c, S->V, nb));
-    CK(dalloc(c, S->fbar[0], nb));
-    CK(dalloc(c, S->fbar[1], nb));
-    CK(dalloc(c, S->sp_tan, (size_t)c->ns));
-    CK(dalloc(c, S->an_tan, 2 * (size_t)c->na));
-    CK(dalloc(c, S->g_spring, (size_t)c->ns));
-    CK(dalloc(c, S->g_angle, (size_t)c->na));
-    CK(dalloc(c, S->diff, 1));
+    CK(ensure(c, S->rec_pos, (size_t)K * nb));
+    CK(ensure(c, S->rec_img, (size_t)K * nb));
+    CK(ensure(c, S->rec_st, (size_t)K * S->st_bytes));
+    const std::vector<int> rb = rebuild_points(S->every, c->grid_update_freq, K);
+    std::vector<int> rb_slot(K);
+    int nrb = 0;
+    for (int j = 0; j < K; ++j) {
+        if (j == 0 || rb[j] != rb[j - 1]) ++nrb;
+        rb_slot[j] = nrb - 1;
+    }
+    CK(ensure(c, S->rec_count, (size_t)nrb * nb));
+    CK(ensure(c, S->rec_list, (size_t)nrb * c->list_stride * c->cfg.list_capacity));
+    CK(ensure(c, S->kmax, 1));
+    CK(ensure(c, S->X, nb));
+    CK(ensure(c, S->V, nb));
+    CK(ensure(c, S->fbar[0], nb));
+    CK(ensure(c, S->fbar[1], nb));
+    CK(ensure(c, S->sp_tan, (size_t)c->ns));
+    CK(ensure(c, S->an_tan, 2 * (size_t)c->na));
+    CK(ensure(c, S->g_spring, (size_t)c->ns));
+    CK(ensure(c, S->g_angle, (size_t)c->na));
+    CK(ensure(c, S->diff, 1));
     const size_t nlam = (size_t)S->nsamples * c->n_nets * 3;
-    CK(dalloc(c, S->lam, nlam));
+    CK(ensure(c, S->lam, nlam));
     CK(cudaMemcpyAsync(S->lam.p, dloss_dreaction, nlam * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(S->g_spring.p, 0, sizeof(double2) * S->g_spring.n, c->stream));
     CK(cudaMemsetAsync(S->g_angle.p, 0, sizeof(double) * S->g_angle.n, c->stream));
@@ -733,7 +877,6 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
         if (j < 0 || (j + 1) % every != 0) return nullptr;
         return S->lam.p + (size_t)((j + 1) / every - 1) * c->n_nets * 3;
     };
-    const std::vector<int> rb = rebuild_points(every, c->grid_update_freq, K);
     const int nbond = (int)(c->ns + c->na);
     int parity = 0;
     {
@@ -746,15 +889,11 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
     for (int q = S->nckpt - 1; q >= 0; --q) {
         r = replay_segment(c, q);
         if (r) return r;
-        int list_from = -1;
         for (int jl = K - 1; jl >= 0; --jl) {
             const long long j = (long long)q * K + jl;
-            if (rb[jl] != list_from) {
-                r = rebuild_from(c, S->rec_pos.p + (size_t)rb[jl] * nb);
-                if (r) return r;
-                list_from = rb[jl];
-            }
             fn::AdjArgs A = adj_args(c, jl, parity);
+            A.list_count = S->rec_count.p + (size_t)rb_slot[jl] * nb;
+            A.list = S->rec_list.p + (size_t)rb_slot[jl] * c->list_stride * c->cfg.list_capacity;
             A.lam_next = lam_at(j - 1);
             if (nbond > 0) {
                 fn::k_adj_bonds<<<(nbond + 255) / 256, 256, 0, c->stream>>>(A);
@@ -799,10 +938,6 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
             grad_vel0[3 * i + 2] = V[q].z;
         }
     }
-    /* the replay buffers are the bulk of the memory: release them */
-    dfree(c, S->rec_pos);
-    dfree(c, S->rec_img);
-    dfree(c, S->rec_st);
     return FN_OK;
 }
 

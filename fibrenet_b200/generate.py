@@ -391,3 +391,37 @@ def dense_mat(seed=2, fibres=40000, beads=100, box=(200.0, 200.0, 200.0), k_s=20
     m = chain_model(pts, st, ["C1"], pk, pr, k_s=k_s, k_a=k_a, vel=vel)
     m.meta.update(kind="dense", seed=seed, fibres=fibres, beads=beads)
     return m
+
+
+def fitting_networks(seed=4, n_networks=64, beads_lo=5000, beads_hi=50000, beads=50, z=20.0,
+                     pull=0.01, dt=0.001, k_s=100.0, k_a=10.0):
+    """Networks of the stiffness-fitting problem (config 4 at its default
+    sizes): the tensile geometry of tensile_network scaled down to 5k-50k
+    beads per network (bead counts uniform, fibres of 50 beads, box side
+    1000 sqrt(F / 20000) so the fibre density matches the 1M-bead test),
+    unbreakable HR springs, clamps pulled at 0.01, dt 0.001."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_networks):
+        F = int(rng.integers(beads_lo // beads, beads_hi // beads + 1))
+        side = float(1000.0 * np.sqrt(F / 20000.0))
+        m = tensile_network(seed=int(rng.integers(0, 2**31 - 1)), fibres=F, beads=beads,
+                            box=(side, side, z), z_range=(1.0, z - 1.0), k_s=k_s, k_a=k_a, dt=dt,
+                            clamp_lo=2.0, clamp_hi=side - 2.0, pull=pull)
+        m.s_type[:] = SPRING_HR
+        m.meta.update(kind="fitting", index=k)
+        out.append(m)
+    return out
+
+
+def perturbed_stiffness(models, seed=5, sigma=0.2):
+    """Copies of ``models`` whose spring stiffnesses are multiplied by
+    lognormal(0, sigma) factors (the target of the fitting problem)."""
+    import copy
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in models:
+        t = copy.copy(m)
+        t.s_k = np.asarray(m.s_k, np.float64) * rng.lognormal(0.0, sigma, m.n_springs)
+        out.append(t)
+    return out

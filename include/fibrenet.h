@@ -244,8 +244,9 @@ FN_API int fn_get_stats(fn_ctx* ctx, fn_stats* out);
    pass; segments are recomputed from their checkpoints (checked bit for bit
    against the next checkpoint).  It leaves the state where the forward pass
    ended; any state change in between makes it fail with FN_ERR_STATE.
-   Device memory: 128 B per bead per checkpoint step of replay, 112 B per
-   bead per checkpoint.  fn_adjoint_release frees it. */
+   Device memory, kept between calls until fn_adjoint_release: 112 B per
+   bead per checkpoint; for the replay 64 B per bead per step of a
+   checkpoint interval plus the contact lists of its rebuilds. */
 FN_API int fn_adjoint_forward(fn_ctx* ctx, int nsamples, int every, int checkpoint_every,
                               int reaction_type, double* reaction);
 FN_API int fn_adjoint_backward(fn_ctx* ctx, const double* dloss_dreaction, double* grad_spring_k,

@@ -161,6 +161,28 @@ def test_directional_finite_differences():
 
 
 @pytest.mark.gpu
+def test_straight_start_stays_bounded():
+    """Fibres that start straight at rest (the fitting networks): the angle
+    Jacobian is taken in its regular form, so the position gradients stay
+    bounded and the stiffness gradient follows central differences."""
+    from fibrenet_b200.fitting import ReactionCurve
+    m = pull(seed=41, vel_sigma=0.0)
+    ns, every = 8, 20
+    curve = ReactionCurve(m, ns, every, 40, CR)
+    k0, r0, a0 = (curve.params[k].copy() for k in ("spring_k", "spring_rest", "angle_k"))
+    R = curve.run(k0, r0, a0)
+    w = np.zeros_like(R)
+    w[..., 0] = 1.0
+    gr = curve.sim.adjoint_backward(w)
+    assert np.all(np.isfinite(gr["pos0"])) and np.abs(gr["pos0"]).max() < 1e6
+    d = k0 * 1e-2
+    fd = float(((curve.run(k0 + d, r0, a0) - curve.run(k0 - d, r0, a0)) * w).sum()) / 2.0
+    an = float(gr["spring_k"] @ d)
+    assert abs(fd - an) <= 1e-2 * abs(an), (fd, an)
+    curve.close()
+
+
+@pytest.mark.gpu
 def test_batched_gradients_equal_single():
     ms = [pull(seed=s) for s in (11, 12, 13)]
     ns, every = 4, 20
