@@ -777,6 +777,7 @@ FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint
     if (nsamples <= 0 || every <= 0 || checkpoint_every <= 0 || checkpoint_every % every != 0)
         return fail(c, FN_ERR_ARG, "fn_adjoint_forward: checkpoint_every must be a positive multiple of every");
     if (c->damp) return fail(c, FN_ERR_ARG, "fn_adjoint_forward: damping must be 0 (velocity-dependent forces are not differentiated)");
+    if (c->verlet) return fail(c, FN_ERR_ARG, "fn_adjoint_forward: needs the fixed rebuild cadence (verlet_skin 0)");
     CK(cudaSetDevice(c->cfg.device));
     const long long total = (long long)nsamples * every;
     if (total % checkpoint_every != 0)

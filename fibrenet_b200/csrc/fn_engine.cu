@@ -113,6 +113,8 @@ void free_all(fn_ctx* c) {
     dfree(c, c->cell_fill);
     dfree(c, c->cell_start);
     dfree(c, c->cell_beads);
+    dfree(c, c->ref_img);
+    dfree(c, c->gate);
     dfree(c, c->list_count);
     dfree(c, c->list);
     dfree(c, c->scan_sums);
@@ -161,6 +163,8 @@ int derive_net(fn_ctx* c, const fn_settings& s, FnNet& N, int net_index) {
         N.box[a] = s.box[a];
     }
     N.cutoff_sq = s.cutoff * s.cutoff;
+    N.list_cut_sq = N.cutoff_sq;
+    if (c->cfg.verlet_skin > 0.0) N.list_cut_sq = (s.cutoff + c->cfg.verlet_skin) * (s.cutoff + c->cfg.verlet_skin);
     N.wall_k = s.wall_k;
     N.nx = (int)std::floor(s.box[0] / s.box_unit_cell);
     N.ny = (int)std::floor(s.box[1] / s.box_unit_cell);
@@ -519,6 +523,7 @@ fn::RebuildArgs rebuild_args(fn_ctx* c) {
     R.cell_fill = c->cell_fill.p;
     R.cell_start = c->cell_start.p;
     R.cell_beads = c->cell_beads.p;
+    R.gate = c->verlet ? c->gate.p : nullptr;
     R.list_count = c->list_count.p;
     R.list = c->list.p;
     R.list_stride = c->list_stride;
@@ -546,7 +551,11 @@ int do_rebuild(fn_ctx* c) {
         e1 = next_event(c);
         CK(cudaEventRecord(e0, c->stream));
     }
-    CK(fn::launch_rebuild(R, c->ntiles, c->block, (int)c->nb, c->ncells, c->scan_sums.p, c->stream));
+    if (c->verlet)
+        CK(fn::launch_verlet_rebuild(R, c->tiles.p, c->img[c->cur].p, c->ref_img.p, c->verlet_thresh2, c->gate.p,
+                                     c->ntiles, c->block, (int)c->nb, c->ncells, c->scan_sums.p, c->stream));
+    else
+        CK(fn::launch_rebuild(R, c->ntiles, c->block, (int)c->nb, c->ncells, c->scan_sums.p, c->stream));
     if (c->timing) {
         CK(cudaEventRecord(e1, c->stream));
         c->ev_rebuild.emplace_back(e0, e1);
@@ -585,6 +594,10 @@ int launch_segment(fn_ctx* c, int len, bool tail) {
     int r = do_rebuild(c);
     if (r) return r;
     for (int k = 0; k < len; ++k) {
+        if (c->verlet && k > 0) {
+            r = do_rebuild(c); /* gated: runs only when a bead moved too far */
+            if (r) return r;
+        }
         const bool last = tail && k == len - 1;
         r = launch_one_step(c, !last, tail && k == len - 2);
         if (r) return r;
@@ -623,6 +636,35 @@ int run_segment(fn_ctx* c, int len, bool tail) {
     c->rebuilds_done++;
     const int drifts = tail ? len - 1 : len;
     if (drifts & 1) c->cur = 1 - c->cur;
+    return FN_OK;
+}
+
+/* Displacement-triggered rebuilds: the smallest gap between listing and
+   acting radius that the grid guarantees (a pair outside the 27-cell
+   stencil is at least one cell step away), and the bead displacement that
+   forces a rebuild (0.45 of it: two beads may close in on each other). */
+int verlet_setup(fn_ctx* c) {
+    c->verlet = false;
+    if (!(c->cfg.verlet_skin > 0.0)) return FN_OK;
+    double s_eff = 1e300;
+    for (int k = 0; k < c->n_nets; ++k) {
+        const FnNet& N = c->nets_h[k];
+        const NetHost& h = c->info[k];
+        const double step = std::min({N.step[0], N.step[1], N.step[2]});
+        if (h.any_cut) s_eff = std::min(s_eff, std::min(step - std::sqrt(N.cutoff_sq), c->cfg.verlet_skin));
+        if (h.any_hs) s_eff = std::min(s_eff, std::min(step - 2.0 * h.rmax, h.skin_gap));
+    }
+    if (!(s_eff > 0.0) || s_eff > 1e299)
+        return fail(c, FN_ERR_ARG,
+                    "displacement-triggered rebuilds need a grid cell wider than the cut-off (than two radii "
+                    "for hs pairs) and a positive skin");
+    const double thresh = 0.45 * s_eff;
+    c->verlet_thresh2 = thresh * thresh;
+    if (!c->ref_img.p || c->ref_img.n < (size_t)c->nb) CK(dalloc(c, c->ref_img, (size_t)c->nb));
+    if (!c->gate.p) CK(dalloc(c, c->gate, 1));
+    const int one = 1;
+    CK(cudaMemcpy(c->gate.p, &one, sizeof one, cudaMemcpyHostToDevice));
+    c->verlet = true;
     return FN_OK;
 }
 
@@ -748,17 +790,19 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         }
         /* largest listing radius (squared): cutoff for lj/st, the largest
            radius + the largest skin for hs (kernel.cl:632-650) */
-        double rmax = 0.0, smax = 0.0;
+        double rmax = 0.0, smax = 0.0, gap = 1e300;
         for (int i = 0; i < d.n_beads; ++i) {
             const float rad = (float)d.radius[i];
             const float skin = (float)((double)rad + d.settings.skin_ratio);
             rmax = std::max(rmax, (double)rad);
             smax = std::max(smax, (double)skin);
+            gap = std::min(gap, (double)skin - (double)rad);
         }
+        c->info[k].skin_gap = gap;
         c->info[k].any_cut = any_cut;
         c->info[k].any_hs = any_hs;
         c->info[k].rmax = rmax;
-        N.list_r2_max = list_r2(c->info[k], N.cutoff_sq, smax);
+        N.list_r2_max = list_r2(c->info[k], N.list_cut_sq, smax);
         NetHost& h = c->info[k];
         h.bead_begin = (int)nb;
         h.bead_end = (int)(nb + d.n_beads);
@@ -963,6 +1007,8 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     c->chain = c->cfg.chain_mode != 2 && build_chain(c, sp_ends, sp_type, an_b, an_s);
     int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128);
     if (r) return r;
+    r = verlet_setup(c);
+    if (r) return r;
     CK(cudaStreamSynchronize(c->stream));
     c->steps_done = 0;
     c->rebuilds_done = 0;
@@ -998,6 +1044,11 @@ FN_API int fn_rebuild_contacts(fn_ctx* c) {
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
+    if (c->verlet) {
+        const int one = 1;
+        CK(cudaMemcpyAsync(c->gate.p, &one, sizeof one, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
     return do_rebuild(c);
 }
 
@@ -1062,6 +1113,10 @@ FN_API int fn_set_beads(fn_ctx* c, int field, const double* host) {
     CK(cudaStreamSynchronize(c->stream));
     const long long nb = c->nb;
     if (field == FN_POSITION || field == FN_IMAGE) {
+        if (c->verlet) {
+            const int one = 1;
+            CK(cudaMemcpy(c->gate.p, &one, sizeof one, cudaMemcpyHostToDevice));
+        }
         DevBuf<double4>& b = field == FN_POSITION ? c->pos[c->cur] : c->img[c->cur];
         std::vector<double4> tmp(nb);
         CK(cudaMemcpy(tmp.data(), b.p, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
@@ -1123,11 +1178,17 @@ FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
     CK(cudaMemcpy(c->binfo.p, tmp.data(), sizeof(int4) * nb, cudaMemcpyHostToDevice));
     for (int k = 0; k < c->n_nets; ++k) {
         double smax = 0.0;
-        for (int i = c->info[k].bead_begin; i < c->info[k].bead_end; ++i)
+        double gap = 1e300;
+        for (int i = c->info[k].bead_begin; i < c->info[k].bead_end; ++i) {
             smax = std::max(smax, (double)(float)skin[i]);
-        c->nets_h[k].list_r2_max = list_r2(c->info[k], c->nets_h[k].cutoff_sq, smax);
+            gap = std::min(gap, (double)(float)skin[i] - (double)(float)c->radius_h[i]);
+        }
+        c->info[k].skin_gap = gap;
+        c->nets_h[k].list_r2_max = list_r2(c->info[k], c->nets_h[k].list_cut_sq, smax);
     }
     CK(cudaMemcpy(c->nets.p, c->nets_h.data(), sizeof(FnNet) * c->n_nets, cudaMemcpyHostToDevice));
+    r = verlet_setup(c);
+    if (r) return r;
     return FN_OK;
 }
 
@@ -1388,6 +1449,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     unsigned long long cnt[FN_CNT_N];
     CK(cudaMemcpyAsync(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->verlet) out->rebuilds = (long long)cnt[FN_CNT_REBUILDS];
     out->cell_overflow = (long long)cnt[FN_CNT_CELL_OVERFLOW];
     out->list_overflow = (long long)cnt[FN_CNT_LIST_OVERFLOW];
     if (cnt[FN_CNT_NONFINITE]) c->err = "non-finite force detected";

@@ -35,6 +35,7 @@ struct NetHost {
     double damping;
     bool any_cut, any_hs; /* pair kinds present (listing radius) */
     double rmax;          /* largest radius, as stored */
+    double skin_gap;      /* smallest skin radius - radius over the beads */
 };
 
 struct AdjointState; /* fn_adjoint.cu */
@@ -115,6 +116,12 @@ struct fn_ctx {
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_step, ev_rebuild;
     size_t ev_next = 0;
+
+    /* displacement-triggered rebuilds (cfg.verlet_skin > 0) */
+    bool verlet = false;
+    double verlet_thresh2 = 0.0; /* squared bead displacement that forces a rebuild */
+    DevBuf<double4> ref_img;     /* image positions at the last rebuild */
+    DevBuf<int> gate;            /* 1: rebuild before the next step */
 
     /* bumped by every call that changes the state or the parameters */
     long long state_version = 0;

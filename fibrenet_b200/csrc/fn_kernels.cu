@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fn_detmath.h"
 #include "fn_device.cuh"
 #include "fn_kernels.h"
@@ -856,7 +858,21 @@ __global__ void k_reset_energy(float4* force, float4* vel, float4* vold, int n) 
 /* Contact-list rebuild                                                      */
 
 /* FillGrid's cell computation (kernel.cl:492-501) + per-cell counting. */
+/* Displacement-triggered mode: every rebuild kernel returns at once unless
+   the device gate says a rebuild is due (a null gate always rebuilds). */
+#define FN_GATED(g)                   \
+    if ((g) != nullptr && *(g) == 0) \
+    return
+
+__global__ void k_fill_int(int* p, long long n, int v, const int* gate) {
+    FN_GATED(gate);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
 __global__ void k_cells(const RebuildArgs R) {
+    FN_GATED(R.gate);
     const FnTile t = R.tiles[blockIdx.x];
     const int i = t.begin + (int)threadIdx.x;
     if (i >= t.end) return;
@@ -875,6 +891,7 @@ __global__ void k_cells(const RebuildArgs R) {
 }
 
 __global__ void k_scatter(const RebuildArgs R, int nb) {
+    FN_GATED(R.gate);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
     const int c = R.cell_of[i];
@@ -887,6 +904,7 @@ __global__ void k_scatter(const RebuildArgs R, int nb) {
    would store them in) and drops the ones beyond the cell capacity, like the
    `old < GRID_TAIL_SIZE` test of kernel.cl:503. */
 __global__ void k_cell_sort(const RebuildArgs R, int ncells) {
+    FN_GATED(R.gate);
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     const int n = R.cell_count[c];
@@ -909,46 +927,18 @@ __global__ void k_cell_sort(const RebuildArgs R, int ncells) {
     }
 }
 
-/* Candidate test of BuildContactList (kernel.cl:574-659) for (i, j). */
-__device__ __forceinline__ bool list_candidate(const FnNet& N, const FnPair* __restrict__ pairs,
-                                               double4 pi, int4 bi, double4 pj, int4 bj) {
-    bool collidable = false;
-    if (bi.x != bj.x)
-        collidable = true;
-    else if (abs(bi.y - bj.y) > 1)
-        collidable = true;
-    if (!collidable) return false;
-    double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
-    double length = rx * rx + ry * ry + rz * rz;
-    if (N.list_mi) length = min_image(N, rx, ry, rz, length, N.list_mi);
-    const int pid = N.pair_base + getadress(bi.z, bj.z, N.types_num);
-    const int kind = pairs[pid].kind;
-    if (kind == 1 || kind == 3) {
-        if (length < N.cutoff_sq) return true;
-    }
-    if (kind == 2) {
-        const double si = (double)__int_as_float(bi.w), sj = (double)__int_as_float(bj.w);
-        const double ri = (double)w_radius(pi.w), rj = (double)w_radius(pj.w);
-        const double min_skin = (si > sj) ? sj : si;
-        const double max_radius = (ri > rj) ? ri : rj;
-        const double lim = max_radius + min_skin;
-        if (length < lim * lim) return true;
-    }
-    return false;
-}
-
-/* The rest of BuildContactList's test (kernel.cl:574-586, 630-659) once the
-   (minimum-image) squared distance is known: exclusion of bonded
-   neighbours, then the listing radius of the pair kind.  Same answer as
-   list_candidate. */
+/* BuildContactList's test (kernel.cl:574-586, 630-659) once the (minimum-
+   image) squared distance is known: exclusion of bonded neighbours, then the
+   listing radius of the pair kind (the cut-off, widened by the Verlet skin in
+   displacement-triggered mode; radius + skin radius for hs pairs). */
 __device__ __forceinline__ bool list_accept(const FnNet& N, const FnPair* __restrict__ pairs,
                                             double length, double4 pi, int4 bi, double4 pj,
                                             int4 bj) {
     if (bi.x == bj.x && abs(bi.y - bj.y) <= 1) return false;
     const int kind = pairs[N.pair_base + getadress(bi.z, bj.z, N.types_num)].kind;
-    if (kind == 1 || kind == 3) return length < N.cutoff_sq;
+    if (kind == 1 || kind == 3) return length < N.list_cut_sq;
     if (kind == 2 || kind == 4) {
-        if (kind == 4 && length < N.cutoff_sq) return true;
+        if (kind == 4 && length < N.list_cut_sq) return true;
         const double si = (double)__int_as_float(bi.w), sj = (double)__int_as_float(bj.w);
         const double ri = (double)w_radius(pi.w), rj = (double)w_radius(pj.w);
         const double min_skin = (si > sj) ? sj : si;
@@ -998,6 +988,7 @@ __device__ __forceinline__ void scan_run(const RebuildArgs& R, const FnNet& N, i
    cells of one (dz, dy) row are one contiguous run of the sorted bead array
    unless the row wraps or a cell overflows. */
 __global__ void k_lists(const RebuildArgs R, long long ncells) {
+    FN_GATED(R.gate);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= R.cell_start[ncells]) return; /* beads placed in the grid */
     const int i = R.cell_beads[t];
@@ -1090,7 +1081,8 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& 
 }
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_partials(const int* in, long long n,
-                                                                 int* block_sums) {
+                                                                 int* block_sums, const int* gate) {
+    FN_GATED(gate);
     __shared__ int ws[33];
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
     int s = 0;
@@ -1104,7 +1096,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_partials(const int* in, l
 
 /* One block scans the block sums in chunks, carrying the running total. */
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int* block_sums, int nblocks,
-                                                             int* grand_total) {
+                                                             int* grand_total, const int* gate) {
+    FN_GATED(gate);
     __shared__ int ws[33];
     int carry = 0;
     for (int base = 0; base < nblocks; base += SCAN_THREADS) {
@@ -1119,7 +1112,9 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int* block_sums, int
 }
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int* in, long long n,
-                                                              const int* block_sums, int* out) {
+                                                              const int* block_sums, int* out,
+                                                              const int* gate) {
+    FN_GATED(gate);
     __shared__ int ws[33];
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
     int v[SCAN_ITEMS];
@@ -1235,7 +1230,20 @@ static cudaError_t set_tiled_smem(size_t bytes) {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+/* The dynamic shared-memory limit is an attribute of the kernel on a
+   device, shared by every context of the process: it is only ever raised
+   (a context with smaller tiles must not lower it under another's launch). */
+static bool raise_limit(size_t* table, size_t& bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    if (bytes <= table[dev]) return false;
+    table[dev] = bytes;
+    return true;
+}
+
 cudaError_t prepare_step_tiled(size_t bytes) {
+    static size_t done[64] = {};
+    if (!raise_limit(done, bytes)) return cudaSuccess;
     cudaError_t e;
     if ((e = set_tiled_smem<true, true, true>(bytes))) return e;
     if ((e = set_tiled_smem<true, false, false>(bytes))) return e;
@@ -1273,6 +1281,8 @@ static cudaError_t set_chain_smem(size_t bytes) {
 }
 
 cudaError_t prepare_step_chain(size_t bytes) {
+    static size_t done[64] = {};
+    if (!raise_limit(done, bytes)) return cudaSuccess;
     cudaError_t e;
     if ((e = set_chain_smem<true, true, true, false>(bytes))) return e;
     if ((e = set_chain_smem<true, false, false, false>(bytes))) return e;
@@ -1337,19 +1347,68 @@ long long scan_block_count(long long n) { return (n + SCAN_TILE - 1) / SCAN_TILE
 cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, long long ncells,
                            int* scan_block_sums, cudaStream_t s) {
     cudaError_t e;
-    if ((e = cudaMemsetAsync(R.cell_count, 0, sizeof(int) * (size_t)ncells, s))) return e;
-    if ((e = cudaMemsetAsync(R.cell_fill, 0, sizeof(int) * (size_t)ncells, s))) return e;
+    const unsigned fill_blocks = (unsigned)std::min<long long>(4096, (ncells + 255) / 256 + 1);
+    if (R.gate) {
+        k_fill_int<<<fill_blocks, 256, 0, s>>>(R.cell_count, ncells, 0, R.gate);
+        k_fill_int<<<fill_blocks, 256, 0, s>>>(R.cell_fill, ncells, 0, R.gate);
+    } else {
+        if ((e = cudaMemsetAsync(R.cell_count, 0, sizeof(int) * (size_t)ncells, s))) return e;
+        if ((e = cudaMemsetAsync(R.cell_fill, 0, sizeof(int) * (size_t)ncells, s))) return e;
+    }
     if (ntiles > 0) k_cells<<<ntiles, block, 0, s>>>(R);
     const long long nblk = scan_block_count(ncells);
-    k_scan_partials<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums);
-    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(scan_block_sums, (int)nblk, R.cell_start + ncells);
+    k_scan_partials<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums, R.gate);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(scan_block_sums, (int)nblk, R.cell_start + ncells, R.gate);
     k_scan_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums,
-                                                          R.cell_start);
+                                                          R.cell_start, R.gate);
     if (nb > 0) k_scatter<<<(nb + 255) / 256, 256, 0, s>>>(R, nb);
     k_cell_sort<<<(unsigned)((ncells + 255) / 256), 256, 0, s>>>(R, (int)ncells);
-    if ((e = cudaMemsetAsync(R.list_count, 0, sizeof(int) * (size_t)nb, s))) return e;
+    if (R.gate) {
+        if (nb > 0) k_fill_int<<<(unsigned)std::min(4096, (nb + 255) / 256), 256, 0, s>>>(R.list_count, nb, 0, R.gate);
+    } else {
+        if ((e = cudaMemsetAsync(R.list_count, 0, sizeof(int) * (size_t)nb, s))) return e;
+    }
     /* every bead may sit in the grid; threads past the grid total return */
     if (nb > 0) k_lists<<<(nb + 127) / 128, 128, 0, s>>>(R, ncells);
+    return cudaGetLastError();
+}
+
+/* Displacement mode: raises the gate when a bead has moved more than the
+   threshold since the last rebuild (image positions, so wraps do not count). */
+__global__ void k_disp_check(const FnTile* tiles, const double4* img, const double4* ref, double thresh2,
+                             int* gate) {
+    const FnTile t = tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    const double4 a = img[i], b = ref[i];
+    const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    if (!(dx * dx + dy * dy + dz * dz <= thresh2)) *gate = 1;
+}
+
+/* After a gated rebuild: the new reference positions. */
+__global__ void k_ref_update(const FnTile* tiles, const double4* img, double4* ref, const int* gate) {
+    FN_GATED(gate);
+    const FnTile t = tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    if (i >= t.end) return;
+    ref[i] = img[i];
+}
+
+__global__ void k_gate_clear(int* gate, unsigned long long* counters) {
+    if (*gate) {
+        counters[FN_CNT_REBUILDS] += 1ull;
+        *gate = 0;
+    }
+}
+
+cudaError_t launch_verlet_rebuild(const RebuildArgs& R, const FnTile* tiles, const double4* img,
+                                  double4* ref, double thresh2, int* gate, int ntiles, int block, int nb,
+                                  long long ncells, int* scan_block_sums, cudaStream_t s) {
+    if (ntiles > 0) k_disp_check<<<ntiles, block, 0, s>>>(tiles, img, ref, thresh2, gate);
+    cudaError_t e = launch_rebuild(R, ntiles, block, nb, ncells, scan_block_sums, s);
+    if (e) return e;
+    if (ntiles > 0) k_ref_update<<<ntiles, block, 0, s>>>(tiles, img, ref, gate);
+    k_gate_clear<<<1, 1, 0, s>>>(gate, R.counters);
     return cudaGetLastError();
 }
 

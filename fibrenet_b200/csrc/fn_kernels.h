@@ -139,6 +139,7 @@ struct RebuildArgs {
     int cell_cap;
     unsigned long long* counters;
     int n_nets;
+    const int* gate; /* displacement mode: rebuild only when *gate != 0 */
 };
 
 struct ObserveArgs {
@@ -202,6 +203,10 @@ long long scan_block_count(long long n);
 cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, long long ncells,
                            int* scan_block_sums, cudaStream_t s);
 cudaError_t launch_observe(const ObserveArgs& O, int nblocks, double* out, cudaStream_t s);
+/* displacement-triggered rebuild: check, gated rebuild, new reference, clear */
+cudaError_t launch_verlet_rebuild(const RebuildArgs& R, const FnTile* tiles, const double4* img,
+                                  double4* ref, double thresh2, int* gate, int ntiles, int block, int nb,
+                                  long long ncells, int* scan_block_sums, cudaStream_t s);
 
 }  // namespace fn
 

@@ -35,6 +35,8 @@ struct FnNet {
     int bead_begin, bead_end;
     int pad_;
     double list_r2_max; /* no pair further apart than this (squared) is listed */
+    double list_cut_sq; /* listing radius of cut-off pair kinds (squared): the
+                           cut-off, plus the Verlet skin in displacement mode */
 };
 
 /* Pair coefficients c1..c6 (SimulationManager.cpp:891-932) and kind. */
@@ -53,6 +55,7 @@ struct FnTile {
 };
 
 /* Device counters (unsigned long long). */
-enum { FN_CNT_CELL_OVERFLOW = 0, FN_CNT_LIST_OVERFLOW = 1, FN_CNT_NONFINITE = 2, FN_CNT_N = 4 };
+enum { FN_CNT_CELL_OVERFLOW = 0, FN_CNT_LIST_OVERFLOW = 1, FN_CNT_NONFINITE = 2, FN_CNT_REBUILDS = 3,
+       FN_CNT_N = 4 };
 
 #endif

@@ -47,7 +47,7 @@ class FnNetworkDesc(C.Structure):
 class FnConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("cell_capacity", C.c_int), ("list_capacity", C.c_int),
                 ("reorder", C.c_int), ("use_graphs", C.c_int), ("block_size", C.c_int),
-                ("chain_mode", C.c_int)]
+                ("chain_mode", C.c_int), ("verlet_skin", C.c_double)]
 
 
 class FnStats(C.Structure):
@@ -197,11 +197,11 @@ class Simulation:
 
     def __init__(self, models, device: int = 0, cell_capacity: int = 64, list_capacity: int = 64,
                  reorder: bool = True, use_graphs: bool = False, block_size: int = 0,
-                 chain: bool = True):
+                 chain: bool = True, verlet_skin: float = 0.0):
         self.lib = load()
         self.models = [models] if isinstance(models, Model) else list(models)
         cfg = FnConfig(device, cell_capacity, list_capacity, int(reorder), int(use_graphs),
-                       block_size, 0 if chain else 2)
+                       block_size, 0 if chain else 2, float(verlet_skin))
         h = C.c_void_p()
         rc = self.lib.fn_create(C.byref(cfg), C.byref(h))
         if rc != FN_OK:

@@ -117,6 +117,17 @@ typedef struct fn_config {
     int block_size;     /* threads per block for the step kernel; 0 = default */
     int chain_mode;     /* 0 auto: per-bead bond records when the model is in
                            chain form (fibres); 2 never (incidence lists) */
+    double verlet_skin; /* 0: the reference's cadence (rebuild every
+                           grid_update_freq steps, counter local to each
+                           fn_step call, SimulationManager.cpp:152-173).
+                           > 0: cut-off pairs are listed out to cutoff + skin
+                           and the list is rebuilt only when some bead has
+                           moved more than 0.45 of the smallest skin (this one
+                           for cut-off kinds, skin radius - radius for hs
+                           kinds, both capped by the cell step minus the
+                           acting radius) since the last rebuild, checked on
+                           the device before every step: no pair within reach
+                           is ever missed.  Not a reference mode. */
 } fn_config;
 
 /* Counters read back from the device. */
