@@ -447,6 +447,9 @@ bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<
 }
 
 int set_block(fn_ctx* c, int block) {
+    if (c->chain && block > fn::kChainMaxBlock)
+        return fail(c, FN_ERR_ARG, "block size " + std::to_string(block) + ": the chain step kernel takes at most " +
+                                       std::to_string(fn::kChainMaxBlock) + " threads per block");
     drop_graphs(c);
     std::vector<FnTile> t;
     int n = build_tiles(c, block, t);
@@ -1592,6 +1595,7 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     for (int b : candidates) {
+        if (c->chain && b > fn::kChainMaxBlock) continue;
         if ((r = set_block(c, b))) break;
         for (int rep = 0; rep < 2 && !r; ++rep) { /* first run warms up */
             c->cur = cur0;

@@ -558,7 +558,12 @@ __device__ __forceinline__ int block_scan_any(int v, int* warp_sums, int& total)
    thread.  FORCES_ONLY evaluates the selected terms alone (no base force, no
    kick or drift, no status change). */
 template <bool DAMP, bool DRIFT, bool STORE_V, bool FORCES_ONLY>
-__global__ void __launch_bounds__(512) k_step_chain(const StepArgs A, int terms) {
+/* At most 256 threads per block and 5 such blocks per SM, i.e. at most 48
+   registers (a few spilled): the kernel waits on dependent loads of contact
+   partners, and the extra resident warps pay (measured on the 1M-bead
+   tensile network: 0.160 vs 0.168 ms per step at the 64 registers of an
+   unbounded build; 40 registers spill too much). */
+__global__ void __launch_bounds__(kChainMaxBlock, 5) k_step_chain(const StepArgs A, int terms) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
     const FnTile tile = A.tiles[blockIdx.x];
     const int b0 = tile.begin, n = tile.end - tile.begin;
@@ -987,7 +992,11 @@ __device__ __forceinline__ void scan_run(const RebuildArgs& R, const FnNet& N, i
    order, so neighbouring threads share their candidate cells; the three
    cells of one (dz, dy) row are one contiguous run of the sorted bead array
    unless the row wraps or a cell overflows. */
-__global__ void k_lists(const RebuildArgs R, long long ncells) {
+/* 12 blocks of 128 per SM (at most 40 registers, a few spilled): the scan
+   waits on dependent loads, and the extra resident warps hide more of that
+   latency than the spills cost (measured: 0.355 vs 0.373 ms per 1M-bead
+   rebuild at the 54 registers the compiler picks unbounded). */
+__global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long long ncells) {
     FN_GATED(R.gate);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= R.cell_start[ncells]) return; /* beads placed in the grid */

@@ -69,6 +69,9 @@ inline size_t step_tiled_smem(int max_sp, int max_an) {
            (size_t)max_sp + (size_t)max_an + 16;
 }
 
+/* largest block the chain step kernel is built for (its launch bounds) */
+constexpr int kChainMaxBlock = 256;
+
 /* chain flag bits */
 enum {
     FN_CH_SPRING = 1,      /* bead has a spring to bead j+1 */

@@ -114,7 +114,8 @@ typedef struct fn_config {
     int list_capacity;  /* contacts kept per bead (full list) */
     int reorder;        /* 1: renumber beads in Morton order of their fibre */
     int use_graphs;     /* 1: replay steps as CUDA graphs */
-    int block_size;     /* threads per block for the step kernel; 0 = default */
+    int block_size;     /* threads per block for the step kernel; 0 = default
+                           (128); at most 256 on the chain path */
     int chain_mode;     /* 0 auto: per-bead bond records when the model is in
                            chain form (fibres); 2 never (incidence lists) */
     double verlet_skin; /* 0: the reference's cadence (rebuild every
