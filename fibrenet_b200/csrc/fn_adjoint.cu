@@ -841,6 +841,8 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
         return fail(c, FN_ERR_STATE, "fn_adjoint_backward: no forward pass matches the current state");
     if (!dloss_dreaction) return fail(c, FN_ERR_ARG, "fn_adjoint_backward: null loss gradient");
     CK(cudaSetDevice(c->cfg.device));
+    r = ensure_incidence(c);
+    if (r) return r;
     const size_t nb = (size_t)c->nb;
     const int K = S->ckpt_every;
     CK(ensure(c, S->rec_pos, (size_t)K * nb));

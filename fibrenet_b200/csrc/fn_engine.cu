@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -17,7 +18,9 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <memory>
 #include <numeric>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -62,6 +65,44 @@ namespace fnh {
 int fail(fn_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
+}
+
+/* Host staging array left uninitialised (every element is written before
+   use): a zero-filled std::vector would touch each page once more, in one
+   thread, before the parallel fill does. */
+template <class T>
+struct HostArray {
+    std::unique_ptr<T[]> p;
+    size_t n = 0;
+    explicit HostArray(size_t count) : p(new T[count ? count : 1]), n(count) {}
+    T& operator[](size_t i) { return p[i]; }
+    const T& operator[](size_t i) const { return p[i]; }
+};
+
+/* Runs f(begin, end) over [0, n) on up to 32 host threads (the upload's
+   conversions are independent per element). */
+template <class F>
+void parallel_for(long long n, F f) {
+    const long long min_chunk = 1 << 15;
+    long long nt = std::min<long long>(32, std::max(1u, std::thread::hardware_concurrency()));
+    nt = std::max(1LL, std::min(nt, (n + min_chunk - 1) / min_chunk));
+    if (nt <= 1) {
+        f(0LL, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const long long chunk = (n + nt - 1) / nt;
+    for (long long t = 0; t < nt; ++t) {
+        const long long b = t * chunk, e = std::min(n, b + chunk);
+        if (b < e) th.emplace_back([=] { f(b, e); });
+    }
+    for (auto& x : th) x.join();
+}
+
+template <class T>
+cudaError_t h2d(fn_ctx* c, DevBuf<T>& b, const HostArray<T>& v) {
+    if (v.n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(b.p, v.p.get(), sizeof(T) * v.n, cudaMemcpyHostToDevice, c->stream);
 }
 
 template <class T>
@@ -259,7 +300,11 @@ void network_order(const fn_network_desc& d, const FnNet& N, bool reorder, std::
     }
     std::vector<int> root(n);
     for (int i = 0; i < n; ++i) root[i] = find(i);
-    std::vector<uint64_t> key(n);
+    /* components (roots = their lowest bead) sorted by the Morton code of
+       their first bead, ties by index; then every component's beads in
+       ascending order: a stable sort of the beads by (key of root, index)
+       done as a counting sort in O(n + R log R) */
+    std::vector<uint64_t> keys;
     for (int i = 0; i < n; ++i) {
         if (root[i] != i) continue;
         uint32_t q[3];
@@ -270,13 +315,19 @@ void network_order(const fn_network_desc& d, const FnNet& N, bool reorder, std::
             q[a] = (uint32_t)x;
         }
         uint64_t m = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
-        key[i] = (m << 32) | (uint32_t)i;
+        keys.push_back((m << 32) | (uint32_t)i);
     }
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        uint64_t ka = key[root[a]], kb = key[root[b]];
-        if (ka != kb) return ka < kb;
-        return a < b;
-    });
+    std::sort(keys.begin(), keys.end());
+    std::vector<int> start(n, 0); /* per root: first output slot */
+    for (int i = 0; i < n; ++i) start[root[i]]++;
+    int acc = 0;
+    for (uint64_t k : keys) {
+        const int r = (int)(uint32_t)k;
+        const int cnt = start[r];
+        start[r] = acc;
+        acc += cnt;
+    }
+    for (int i = 0; i < n; ++i) order[start[root[i]]++] = i;
 }
 
 int build_tiles(fn_ctx* c, int block, std::vector<FnTile>& out) {
@@ -410,32 +461,44 @@ bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<
             if (!((ss.x == sp && ss.y == sn) || (ss.x == sn && ss.y == sp))) return false;
         }
     }
-    for (long long i = 0; i < nb; ++i) {
-        if (i > 0 && next_sp[i - 1] >= 0 && next_sp[i] >= 0 && next_sp[i - 1] > next_sp[i]) return false;
-        int last = -1;
-        for (long long q = i - 1; q <= i + 1; ++q) {
-            if (q < 0 || q >= nb || centre_an[q] < 0) continue;
-            if (centre_an[q] < last) return false;
-            last = centre_an[q];
+    std::atomic<bool> bad{false};
+    parallel_for(nb, [&](long long i0, long long i1) {
+        for (long long i = i0; i < i1; ++i) {
+            if (i > 0 && next_sp[i - 1] >= 0 && next_sp[i] >= 0 && next_sp[i - 1] > next_sp[i]) bad = true;
+            int last = -1;
+            for (long long q = i - 1; q <= i + 1; ++q) {
+                if (q < 0 || q >= nb || centre_an[q] < 0) continue;
+                if (centre_an[q] < last) bad = true;
+                last = centre_an[q];
+            }
         }
-    }
-    std::vector<float4> chs(nb, make_float4(0, 0, 0, 0));
-    std::vector<float2> cha(nb, make_float2(0, 0));
-    std::vector<unsigned char> st(nb, 0);
-    c->sp_bead.assign(c->ns, 0);
-    c->an_bead.assign(c->na, 0);
-    for (long long i = 0; i < nb; ++i) {
-        if (next_sp[i] >= 0) {
-            chs[i] = c->sp_par_h[next_sp[i]];
-            c->sp_bead[next_sp[i]] = (int)i;
-            st[i] |= 1;
+    });
+    if (bad) return false;
+    HostArray<float4> chs(nb);
+    HostArray<float2> cha(nb);
+    HostArray<unsigned char> st(nb);
+    c->sp_bead.resize(c->ns);
+    c->an_bead.resize(c->na);
+    /* each spring is the next spring of exactly one bead and each angle is
+       centred on exactly one: the scattered writes below never collide */
+    parallel_for(nb, [&](long long i0, long long i1) {
+        for (long long i = i0; i < i1; ++i) {
+            chs[i] = make_float4(0, 0, 0, 0);
+            cha[i] = make_float2(0, 0);
+            unsigned char b = 0;
+            if (next_sp[i] >= 0) {
+                chs[i] = c->sp_par_h[next_sp[i]];
+                c->sp_bead[next_sp[i]] = (int)i;
+                b |= 1;
+            }
+            if (centre_an[i] >= 0) {
+                cha[i] = c->an_par_h[centre_an[i]];
+                c->an_bead[centre_an[i]] = (int)i;
+                b |= 2;
+            }
+            st[i] = b;
         }
-        if (centre_an[i] >= 0) {
-            cha[i] = c->an_par_h[centre_an[i]];
-            c->an_bead[centre_an[i]] = (int)i;
-            st[i] |= 2;
-        }
-    }
+    });
     if (dalloc(c, c->ch_sp, nb) || dalloc(c, c->ch_an, nb) || dalloc(c, c->ch_flags, nb) ||
         dalloc(c, c->ch_status, nb))
         return false;
@@ -444,6 +507,60 @@ bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<
         return false;
     c->ch_flags_h = fl;
     return true;
+}
+
+/* Bead -> bond incidence (CSR, ascending bond index per bead), built on
+   first need: the incidence step kernels, the per-tile term lists and the
+   adjoint read it; the chain step kernel does not, so chain-form models skip
+   it at upload. */
+int ensure_incidence(fn_ctx* c) {
+    if (c->incidence_ready) return FN_OK;
+    const long long nb = c->nb, ns = c->ns, na = c->na;
+    const std::vector<int2>& sp_ends = c->sp_ends_h;
+    const std::vector<int4>& an_b = c->an_b_h;
+    std::vector<int> sp_off(nb + 1, 0), an_off(nb + 1, 0);
+    for (long long s = 0; s < ns; ++s) {
+        sp_off[sp_ends[s].x + 1]++;
+        sp_off[sp_ends[s].y + 1]++;
+    }
+    for (long long a = 0; a < na; ++a) {
+        an_off[an_b[a].x + 1]++;
+        an_off[an_b[a].y + 1]++;
+        an_off[an_b[a].z + 1]++;
+    }
+    for (long long i = 0; i < nb; ++i) {
+        sp_off[i + 1] += sp_off[i];
+        an_off[i + 1] += an_off[i];
+    }
+    std::vector<int> sp_ent(2 * ns), an_ent(3 * na);
+    {
+        std::vector<int> fill(sp_off.begin(), sp_off.end() - 1);
+        for (long long s = 0; s < ns; ++s) {
+            sp_ent[fill[sp_ends[s].x]++] = (int)(s << 1);
+            sp_ent[fill[sp_ends[s].y]++] = (int)((s << 1) | 1);
+        }
+        std::vector<int> fa(an_off.begin(), an_off.end() - 1);
+        for (long long a = 0; a < na; ++a) {
+            an_ent[fa[an_b[a].x]++] = (int)(a << 2);
+            an_ent[fa[an_b[a].y]++] = (int)((a << 2) | 1);
+            an_ent[fa[an_b[a].z]++] = (int)((a << 2) | 2);
+        }
+    }
+    c->sp_off_h = std::move(sp_off);
+    c->sp_ent_h = std::move(sp_ent);
+    c->an_off_h = std::move(an_off);
+    c->an_ent_h = std::move(an_ent);
+    CK(dalloc(c, c->sp_off, nb + 1));
+    CK(dalloc(c, c->sp_ent, 2 * ns));
+    CK(dalloc(c, c->an_off, nb + 1));
+    CK(dalloc(c, c->an_ent, 3 * na));
+    CK(h2d(c, c->sp_off, c->sp_off_h));
+    CK(h2d(c, c->sp_ent, c->sp_ent_h));
+    CK(h2d(c, c->an_off, c->an_off_h));
+    CK(h2d(c, c->an_ent, c->an_ent_h));
+    CK(cudaStreamSynchronize(c->stream));
+    c->incidence_ready = true;
+    return FN_OK;
 }
 
 int set_block(fn_ctx* c, int block) {
@@ -459,7 +576,9 @@ int set_block(fn_ctx* c, int block) {
     if (c->chain) {
         CK(fn::prepare_step_chain(fn::step_chain_smem(block)));
     } else {
-        int r = build_tile_terms(c, t);
+        int r = ensure_incidence(c);
+        if (r) return r;
+        r = build_tile_terms(c, t);
         if (r) return r;
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -851,15 +970,16 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     }
 
     /* bead arrays in internal order */
-    std::vector<double4> pos(nb), img(nb);
-    std::vector<float4> vold(nb), force(nb), vel(nb);
-    std::vector<int4> binfo(nb);
-    c->mass_h.assign(nb, 0.0);
-    c->radius_h.assign(nb, 0.0);
+    HostArray<double4> pos(nb), img(nb);
+    HostArray<float4> vold(nb), force(nb), vel(nb);
+    HostArray<int4> binfo(nb);
+    c->mass_h.resize(nb);
+    c->radius_h.resize(nb);
     for (int k = 0; k < n_networks; ++k) {
         const fn_network_desc& d = nets[k];
         const int base = c->info[k].bead_begin;
-        for (int i = 0; i < d.n_beads; ++i) {
+        parallel_for(d.n_beads, [&](long long i0, long long i1) {
+        for (int i = (int)i0; i < (int)i1; ++i) {
             const int q = c->inv[base + i];
             const float rad = (float)d.radius[i];
             const double mass = d.mass[i];
@@ -876,6 +996,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
             const float skin = (float)((double)rad + d.settings.skin_ratio);
             binfo[q] = make_int4(d.tag[i], d.loc_id[i], d.type[i], float_bits(skin));
         }
+        });
     }
 
     /* springs and angles keep their (concatenated) file order */
@@ -889,13 +1010,16 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     for (int k = 0; k < n_networks; ++k) {
         const fn_network_desc& d = nets[k];
         const NetHost& h = c->info[k];
-        for (int s = 0; s < d.n_springs; ++s) {
+        parallel_for(d.n_springs, [&](long long s0, long long s1) {
+        for (int s = (int)s0; s < (int)s1; ++s) {
             const int g = h.spring_begin + s;
             sp_ends[g] = make_int2(c->inv[h.bead_begin + d.s_p1[s]], c->inv[h.bead_begin + d.s_p2[s]]);
             sp_type[g] = (signed char)d.s_type[s];
             c->sp_par_h[g] = make_float4((float)d.s_rest[s], (float)d.s_k[s], (float)d.s_c1[s], (float)d.s_c2[s]);
         }
-        for (int a = 0; a < d.n_angles; ++a) {
+        });
+        parallel_for(d.n_angles, [&](long long a0, long long a1) {
+        for (int a = (int)a0; a < (int)a1; ++a) {
             const int g = h.angle_begin + a;
             an_b[g] = make_int4(c->inv[h.bead_begin + d.a_b1[a]], c->inv[h.bead_begin + d.a_b2[a]],
                                 c->inv[h.bead_begin + d.a_b3[a]], d.a_type[a]);
@@ -904,42 +1028,11 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
             an_s[g] = make_int2(s1, s2);
             c->an_par_h[g] = make_float2((float)d.a_theta0[a], (float)d.a_k[a]);
         }
+        });
     }
 
-    /* bead -> bond incidence, ascending bond index per bead */
-    std::vector<int> sp_off(nb + 1, 0), an_off(nb + 1, 0);
-    for (long long s = 0; s < ns; ++s) {
-        sp_off[sp_ends[s].x + 1]++;
-        sp_off[sp_ends[s].y + 1]++;
-    }
-    for (long long a = 0; a < na; ++a) {
-        an_off[an_b[a].x + 1]++;
-        an_off[an_b[a].y + 1]++;
-        an_off[an_b[a].z + 1]++;
-    }
-    for (long long i = 0; i < nb; ++i) {
-        sp_off[i + 1] += sp_off[i];
-        an_off[i + 1] += an_off[i];
-    }
-    std::vector<int> sp_ent(2 * ns), an_ent(3 * na);
-    {
-        std::vector<int> fill(sp_off.begin(), sp_off.end() - 1);
-        for (long long s = 0; s < ns; ++s) {
-            sp_ent[fill[sp_ends[s].x]++] = (int)(s << 1);
-            sp_ent[fill[sp_ends[s].y]++] = (int)((s << 1) | 1);
-        }
-        std::vector<int> fa(an_off.begin(), an_off.end() - 1);
-        for (long long a = 0; a < na; ++a) {
-            an_ent[fa[an_b[a].x]++] = (int)(a << 2);
-            an_ent[fa[an_b[a].y]++] = (int)((a << 2) | 1);
-            an_ent[fa[an_b[a].z]++] = (int)((a << 2) | 2);
-        }
-    }
-
-    c->sp_off_h = sp_off;
-    c->sp_ent_h = sp_ent;
-    c->an_off_h = an_off;
-    c->an_ent_h = an_ent;
+    c->sp_ends_h = sp_ends;
+    c->incidence_ready = false;
     c->an_b_h = an_b;
     c->an_s_h = an_s;
     c->list_stride = (int)((nb + 31) / 32 * 32);
@@ -960,10 +1053,6 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     CK(dalloc(c, c->an_s, na));
     CK(dalloc(c, c->an_par, na));
     CK(dalloc(c, c->an_status, na));
-    CK(dalloc(c, c->sp_off, nb + 1));
-    CK(dalloc(c, c->sp_ent, 2 * ns));
-    CK(dalloc(c, c->an_off, nb + 1));
-    CK(dalloc(c, c->an_ent, 3 * na));
     CK(dalloc(c, c->cell_of, nb));
     CK(dalloc(c, c->cell_count, ncells));
     CK(dalloc(c, c->cell_fill, ncells));
@@ -983,8 +1072,8 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     c->cur = 0;
     CK(h2d(c, c->pos[0], pos));
     CK(h2d(c, c->img[0], img));
-    CK(h2d(c, c->pos[1], pos));
-    CK(h2d(c, c->img[1], img));
+    CK(cudaMemcpyAsync(c->pos[1].p, c->pos[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->img[1].p, c->img[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
     CK(h2d(c, c->vold, vold));
     CK(h2d(c, c->force, force));
     CK(h2d(c, c->vel, vel));
@@ -997,10 +1086,6 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     CK(h2d(c, c->an_s, an_s));
     CK(h2d(c, c->an_par, c->an_par_h));
     CK(h2d(c, c->an_status, an_status));
-    CK(h2d(c, c->sp_off, sp_off));
-    CK(h2d(c, c->sp_ent, sp_ent));
-    CK(h2d(c, c->an_off, an_off));
-    CK(h2d(c, c->an_ent, an_ent));
     CK(h2d(c, c->nets, c->nets_h));
     CK(h2d(c, c->pairs, c->pairs_h));
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * FN_CNT_N, c->stream));

@@ -79,6 +79,8 @@ struct fn_ctx {
     /* host copies of the incidence (internal numbering) for the tile lists */
     std::vector<int> sp_off_h, sp_ent_h, an_off_h, an_ent_h;
     std::vector<int4> an_b_h;
+    std::vector<int2> sp_ends_h;  /* internal bead numbering */
+    bool incidence_ready = false; /* sp_off/sp_ent/an_off/an_ent built (on first need) */
     std::vector<int2> an_s_h;
     /* per-tile bonded term lists of the tiled step kernel */
     DevBuf<int> tile_sp_off, tile_sp, tile_an_off, tile_an, sp_slot, an_slot;
@@ -169,6 +171,7 @@ void dfree(fn_ctx* c, DevBuf<T>& b) {
 }
 
 int check_ready(fn_ctx* c);
+int ensure_incidence(fn_ctx* c);
 fn::StepArgs step_args(fn_ctx* c, bool pingpong);
 fn::RebuildArgs rebuild_args(fn_ctx* c);
 void drop_graphs(fn_ctx* c);
