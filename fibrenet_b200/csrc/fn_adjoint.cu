@@ -244,6 +244,7 @@ struct AdjArgs {
     int list_stride, list_cap;
     int ns, na;
     /* adjoint state */
+    const double* minv; /* 1/mass per bead (0 for mass 0), the image positions' w */
     float4* X;
     float4* V;
     const float4* fbar;    /* Fbar of evaluation j */
@@ -343,16 +344,18 @@ __global__ void __launch_bounds__(512) k_adj_beads(const AdjArgs A) {
     for (int e = A.an_off[i]; e < A.an_off[i + 1]; ++e) {
         const int ent = A.an_ent[e];
         const int q = ent >> 2, role = ent & 3;
-        const float4 t1 = A.an_tan[2 * (size_t)q], t3 = A.an_tan[2 * (size_t)q + 1];
         if (role == 0) {
+            const float4 t1 = A.an_tan[2 * (size_t)q];
             jx += t1.x;
             jy += t1.y;
             jz += t1.z;
         } else if (role == 2) {
+            const float4 t3 = A.an_tan[2 * (size_t)q + 1];
             jx += t3.x;
             jy += t3.y;
             jz += t3.z;
         } else {
+            const float4 t1 = A.an_tan[2 * (size_t)q], t3 = A.an_tan[2 * (size_t)q + 1];
             jx -= (double)t1.x + (double)t3.x;
             jy -= (double)t1.y + (double)t3.y;
             jz -= (double)t1.z + (double)t3.z;
@@ -387,7 +390,7 @@ __global__ void __launch_bounds__(512) k_adj_beads(const AdjArgs A) {
     X.z = (float)((double)X.z + jz);
     A.X[i] = X;
     /* prologue of evaluation j - 1 */
-    const double minv = A.img[i].w;
+    const double minv = A.minv[i];
     float4 V = A.V[i];
     V.x = (float)((double)V.x + N.dt * (double)X.x);
     V.y = (float)((double)V.y + N.dt * (double)X.y);
@@ -487,6 +490,12 @@ __global__ void k_list_copy(const int* count, const int* list, int n, int stride
     for (int k = 0; k < km; ++k) list_out[(size_t)k * stride + i] = list[(size_t)k * stride + i];
 }
 
+/* 1/mass of every bead, read once from the image positions' w. */
+__global__ void k_take_minv(const double4* img, int n, double* minv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) minv[i] = img[i].w;
+}
+
 /* Counts beads whose positions differ bit-wise between two buffers. */
 __global__ void k_count_diff(const double4* a, const double4* b, int n, unsigned long long* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -522,6 +531,7 @@ struct AdjointState {
     int nchunks = 1;
     /* adjoint */
     DevBuf<float4> X, V, fbar[2], sp_tan, an_tan;
+    DevBuf<double> minv;
     DevBuf<double2> g_spring;
     DevBuf<double> g_angle, lam;
     DevBuf<unsigned long long> diff;
@@ -547,6 +557,7 @@ void adjoint_free(fn_ctx* c) {
     dfree(c, S->kmax);
     dfree(c, S->react_partial);
     dfree(c, S->X);
+    dfree(c, S->minv);
     dfree(c, S->V);
     dfree(c, S->fbar[0]);
     dfree(c, S->fbar[1]);
@@ -751,6 +762,7 @@ fn::AdjArgs adj_args(fn_ctx* c, int j_local, int parity) {
     A.list_cap = c->cfg.list_capacity;
     A.ns = (int)c->ns;
     A.na = (int)c->na;
+    A.minv = S->minv.p;
     A.X = S->X.p;
     A.V = S->V.p;
     A.fbar = S->fbar[parity].p;
@@ -859,6 +871,9 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
     CK(ensure(c, S->rec_list, (size_t)nrb * c->list_stride * c->cfg.list_capacity));
     CK(ensure(c, S->kmax, 1));
     CK(ensure(c, S->X, nb));
+    CK(ensure(c, S->minv, nb));
+    fn::k_take_minv<<<(int)((nb + 255) / 256), 256, 0, c->stream>>>(S->ck_img.p, (int)nb, S->minv.p);
+    CK(cudaGetLastError());
     CK(ensure(c, S->V, nb));
     CK(ensure(c, S->fbar[0], nb));
     CK(ensure(c, S->fbar[1], nb));
