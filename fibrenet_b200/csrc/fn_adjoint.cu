@@ -242,7 +242,7 @@ struct AdjArgs {
     const int* list_count;
     const int* list;
     int list_stride, list_cap;
-    int ns, na;
+    int ns, na, nb;
     /* adjoint state */
     const double* minv; /* 1/mass per bead (0 for mass 0), the image positions' w */
     float4* X;
@@ -251,6 +251,12 @@ struct AdjArgs {
     float4* fbar_next;     /* Fbar of evaluation j - 1 */
     float4* sp_tan;        /* per spring: tangent force on p1 */
     float4* an_tan;        /* per angle: tangent on b1, then on b3 (2 entries) */
+    /* chain form: the same tangents by bead, so a bead reads its neighbours'
+       slots instead of incidence lists: spring (j, j+1) at j as the tangent
+       on bead j; angle centred on j at 2j (on bead j-1) and 2j+1 (on j+1);
+       slots without a bond stay zero */
+    float4* sp_tan_b;
+    float4* an_tan_b;
     double2* g_spring;     /* d loss / d (k, rest) */
     double* g_angle;       /* d loss / d k */
     /* loss injection at evaluation j - 1: per network 3 doubles, or null */
@@ -290,7 +296,14 @@ __global__ void __launch_bounds__(256) k_adj_bonds(const AdjArgs A) {
             g.y += k * ud;
             A.g_spring[s] = g;
         }
-        A.sp_tan[s] = out;
+        if (A.sp_tan_b) {
+            if (e.x < e.y)
+                A.sp_tan_b[e.x] = out;
+            else
+                A.sp_tan_b[e.y] = make_float4(-out.x, -out.y, -out.z, 0.f);
+        } else {
+            A.sp_tan[s] = out;
+        }
         return;
     }
     const int q = t - A.ns;
@@ -318,13 +331,20 @@ __global__ void __launch_bounds__(256) k_adj_bonds(const AdjArgs A) {
         for (int a = 0; a < 3; ++a) g += pa[a].v * (F1[a] - F2[a]) + pc[a].v * (F3[a] - F2[a]);
         A.g_angle[q] += g;
     }
-    A.an_tan[2 * (size_t)q] = o1;
-    A.an_tan[2 * (size_t)q + 1] = o3;
+    if (A.an_tan_b) {
+        const bool fwd = b.x < b.y;
+        A.an_tan_b[2 * (size_t)b.y] = fwd ? o1 : o3;
+        A.an_tan_b[2 * (size_t)b.y + 1] = fwd ? o3 : o1;
+    } else {
+        A.an_tan[2 * (size_t)q] = o1;
+        A.an_tan[2 * (size_t)q + 1] = o3;
+    }
 }
 
 /* Per bead: X += (J Fbar)_i from the bond tangents, the contacts of its
    list and the walls; then the prologue of evaluation j - 1:
    V += dt X, Fbar_{j-1} = (dt/m) V + loss injection. */
+template <bool CHAIN>
 __global__ void __launch_bounds__(512) k_adj_beads(const AdjArgs A) {
     const FnTile tl = A.tiles[blockIdx.x];
     const int i = tl.begin + (int)threadIdx.x;
@@ -333,7 +353,19 @@ __global__ void __launch_bounds__(512) k_adj_beads(const AdjArgs A) {
     const double4 p = A.pos[i];
     const float4 wi = A.fbar[i];
     double jx = 0.0, jy = 0.0, jz = 0.0;
-    for (int e = A.sp_off[i]; e < A.sp_off[i + 1]; ++e) {
+    if (CHAIN) {
+        /* spring (i-1, i), spring (i, i+1); angles centred on i-1, i, i+1 */
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 sp = i > 0 ? A.sp_tan_b[i - 1] : zero;
+        const float4 sn = A.sp_tan_b[i];
+        const float4 ap = i > 0 ? A.an_tan_b[2 * (size_t)(i - 1) + 1] : zero;
+        const float4 c0 = A.an_tan_b[2 * (size_t)i], c1 = A.an_tan_b[2 * (size_t)i + 1];
+        const float4 an = i + 1 < A.nb ? A.an_tan_b[2 * (size_t)(i + 1)] : zero;
+        jx += -(double)sp.x + (double)sn.x + (double)ap.x - ((double)c0.x + (double)c1.x) + (double)an.x;
+        jy += -(double)sp.y + (double)sn.y + (double)ap.y - ((double)c0.y + (double)c1.y) + (double)an.y;
+        jz += -(double)sp.z + (double)sn.z + (double)ap.z - ((double)c0.z + (double)c1.z) + (double)an.z;
+    }
+    for (int e = CHAIN ? 0 : A.sp_off[i]; e < (CHAIN ? 0 : A.sp_off[i + 1]); ++e) {
         const int ent = A.sp_ent[e];
         const float4 t = A.sp_tan[ent >> 1];
         const double sg = (ent & 1) ? -1.0 : 1.0;
@@ -341,7 +373,7 @@ __global__ void __launch_bounds__(512) k_adj_beads(const AdjArgs A) {
         jy += sg * (double)t.y;
         jz += sg * (double)t.z;
     }
-    for (int e = A.an_off[i]; e < A.an_off[i + 1]; ++e) {
+    for (int e = CHAIN ? 0 : A.an_off[i]; e < (CHAIN ? 0 : A.an_off[i + 1]); ++e) {
         const int ent = A.an_ent[e];
         const int q = ent >> 2, role = ent & 3;
         if (role == 0) {
@@ -530,7 +562,7 @@ struct AdjointState {
     DevBuf<double> react_partial;
     int nchunks = 1;
     /* adjoint */
-    DevBuf<float4> X, V, fbar[2], sp_tan, an_tan;
+    DevBuf<float4> X, V, fbar[2], sp_tan, an_tan, sp_tan_b, an_tan_b;
     DevBuf<double> minv;
     DevBuf<double2> g_spring;
     DevBuf<double> g_angle, lam;
@@ -563,6 +595,8 @@ void adjoint_free(fn_ctx* c) {
     dfree(c, S->fbar[1]);
     dfree(c, S->sp_tan);
     dfree(c, S->an_tan);
+    dfree(c, S->sp_tan_b);
+    dfree(c, S->an_tan_b);
     dfree(c, S->g_spring);
     dfree(c, S->g_angle);
     dfree(c, S->lam);
@@ -762,6 +796,11 @@ fn::AdjArgs adj_args(fn_ctx* c, int j_local, int parity) {
     A.list_cap = c->cfg.list_capacity;
     A.ns = (int)c->ns;
     A.na = (int)c->na;
+    A.nb = (int)c->nb;
+    if (c->chain) {
+        A.sp_tan_b = S->sp_tan_b.p;
+        A.an_tan_b = S->an_tan_b.p;
+    }
     A.minv = S->minv.p;
     A.X = S->X.p;
     A.V = S->V.p;
@@ -853,8 +892,10 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
         return fail(c, FN_ERR_STATE, "fn_adjoint_backward: no forward pass matches the current state");
     if (!dloss_dreaction) return fail(c, FN_ERR_ARG, "fn_adjoint_backward: null loss gradient");
     CK(cudaSetDevice(c->cfg.device));
-    r = ensure_incidence(c);
-    if (r) return r;
+    if (!c->chain) { /* the chain form gathers bond tangents by bead */
+        r = ensure_incidence(c);
+        if (r) return r;
+    }
     const size_t nb = (size_t)c->nb;
     const int K = S->ckpt_every;
     CK(ensure(c, S->rec_pos, (size_t)K * nb));
@@ -879,6 +920,12 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
     CK(ensure(c, S->fbar[1], nb));
     CK(ensure(c, S->sp_tan, (size_t)c->ns));
     CK(ensure(c, S->an_tan, 2 * (size_t)c->na));
+    if (c->chain) {
+        CK(ensure(c, S->sp_tan_b, nb));
+        CK(ensure(c, S->an_tan_b, 2 * nb));
+        CK(cudaMemsetAsync(S->sp_tan_b.p, 0, sizeof(float4) * nb, c->stream));
+        CK(cudaMemsetAsync(S->an_tan_b.p, 0, sizeof(float4) * 2 * nb, c->stream));
+    }
     CK(ensure(c, S->g_spring, (size_t)c->ns));
     CK(ensure(c, S->g_angle, (size_t)c->na));
     CK(ensure(c, S->diff, 1));
@@ -917,7 +964,10 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
                 fn::k_adj_bonds<<<(nbond + 255) / 256, 256, 0, c->stream>>>(A);
                 CK(cudaGetLastError());
             }
-            fn::k_adj_beads<<<c->ntiles, c->block, 0, c->stream>>>(A);
+            if (c->chain)
+                fn::k_adj_beads<true><<<c->ntiles, c->block, 0, c->stream>>>(A);
+            else
+                fn::k_adj_beads<false><<<c->ntiles, c->block, 0, c->stream>>>(A);
             CK(cudaGetLastError());
             parity = 1 - parity;
         }
