@@ -1153,6 +1153,29 @@ FN_API int fn_sync(fn_ctx* c) {
     if (!c) return FN_ERR_ARG;
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
+    if (!c->uploaded) return FN_OK;
+    unsigned long long bad = 0;
+    CK(cudaMemcpy(&bad, c->counters.p + FN_CNT_NONFINITE, sizeof bad, cudaMemcpyDeviceToHost));
+    if (bad) return fail(c, FN_ERR_NONFINITE, "non-finite force detected in " + std::to_string(bad) + " bead-steps");
+    return FN_OK;
+}
+
+FN_API int fn_device_view(fn_ctx* c, int field, fn_view* out) {
+    int r = check_ready(c);
+    if (r) return r;
+    if (!out) return fail(c, FN_ERR_ARG, "fn_device_view: null output");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    out->n = c->nb;
+    out->components = 4;
+    switch (field) {
+    case FN_POSITION: out->ptr = c->pos[c->cur].p; out->elem_bytes = 8; break;
+    case FN_IMAGE: out->ptr = c->img[c->cur].p; out->elem_bytes = 8; break;
+    case FN_VELOCITY: out->ptr = c->vel.p; out->elem_bytes = 4; break;
+    case FN_FORCE: out->ptr = c->force.p; out->elem_bytes = 4; break;
+    case FN_VELOCITY_OLD: out->ptr = c->vold.p; out->elem_bytes = 4; break;
+    default: return fail(c, FN_ERR_ARG, "fn_device_view: unknown field");
+    }
     return FN_OK;
 }
 
@@ -1538,6 +1561,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     CK(cudaMemcpyAsync(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (c->verlet) out->rebuilds = (long long)cnt[FN_CNT_REBUILDS];
+    out->nonfinite = (long long)cnt[FN_CNT_NONFINITE];
     out->cell_overflow = (long long)cnt[FN_CNT_CELL_OVERFLOW];
     out->list_overflow = (long long)cnt[FN_CNT_LIST_OVERFLOW];
     if (cnt[FN_CNT_NONFINITE]) c->err = "non-finite force detected";

@@ -54,7 +54,13 @@ class FnStats(C.Structure):
     _fields_ = [("cell_overflow", C.c_longlong), ("list_overflow", C.c_longlong),
                 ("rebuilds", C.c_longlong), ("steps", C.c_longlong), ("block_size", C.c_int),
                 ("bond_path", C.c_int), ("n_networks", C.c_int), ("n_beads", C.c_longlong),
-                ("device_bytes", C.c_longlong), ("graph_launches", C.c_longlong)]
+                ("device_bytes", C.c_longlong), ("graph_launches", C.c_longlong),
+                ("nonfinite", C.c_longlong)]
+
+
+class FnView(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("n", C.c_longlong), ("elem_bytes", C.c_int),
+                ("components", C.c_int)]
 
 
 class FnObservables(C.Structure):
@@ -102,6 +108,7 @@ SIGNATURES = {
     "fn_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FnStats)]),
     "fn_observe_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "fn_energy_eval": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FnEnergy)]),
+    "fn_device_view": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FnView)]),
     "fn_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _D]),
     "fn_adjoint_backward": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D, _D]),
     "fn_adjoint_release": (C.c_int, [C.c_void_p]),
@@ -207,6 +214,7 @@ class Simulation:
         if rc != FN_OK:
             raise NativeError(rc, "fn_create failed (no CUDA device or bad config)")
         self.h = h
+        self.device = device
         self.list_capacity = list_capacity
         keep = _Keep()
         descs = (FnNetworkDesc * len(self.models))(*[network_desc(m, keep) for m in self.models])
@@ -330,6 +338,22 @@ class Simulation:
         self._check(self.lib.fn_step_series(self.h, nsteps, every, net, reaction_type, int(energy),
                                             out.ctypes.data_as(_D)))
         return out
+
+    def device_view(self, field: str):
+        """The device array of ``field`` as a torch tensor [n, 4] without a
+        copy (internal bead order, see permutation()); valid until the next
+        step, upload or state restore."""
+        import torch
+        v = FnView()
+        self._check(self.lib.fn_device_view(self.h, FIELDS[field], C.byref(v)))
+
+        class _Iface:
+            pass
+        it = _Iface()
+        it.__cuda_array_interface__ = {
+            "shape": (int(v.n), int(v.components)), "typestr": "<f8" if v.elem_bytes == 8 else "<f4",
+            "data": (int(v.ptr), False), "version": 3, "strides": None}
+        return torch.as_tensor(it, device=f"cuda:{self.device}")
 
     # --- differentiation
     def adjoint_forward(self, nsamples: int, every: int, checkpoint_every: int,

@@ -143,7 +143,21 @@ typedef struct fn_stats {
     long long n_beads;
     long long device_bytes;    /* device memory held by the context */
     long long graph_launches;  /* step segments replayed as CUDA graphs */
+    long long nonfinite;       /* bead-steps whose new force was NaN or inf */
 } fn_stats;
+
+/* A device array of the context, for zero-copy readers (torch through
+   __cuda_array_interface__).  Beads are in internal order (fn_get_permutation)
+   with 4 components per bead (the 4th is packing: radius/type bits for
+   positions, 1/mass for images, 0 for velocities and forces).  The pointer is
+   valid until the next call that steps, uploads or restores state: positions
+   alternate between two buffers from step to step. */
+typedef struct fn_view {
+    void* ptr;
+    long long n;    /* beads */
+    int elem_bytes; /* bytes of one component: 8 (FP64) or 4 (FP32) */
+    int components; /* 4 */
+} fn_view;
 
 /* Per-network observables (FP64 reductions on the device). */
 typedef struct fn_observables {
@@ -200,6 +214,8 @@ FN_API int fn_rebuild_contacts(fn_ctx* ctx);
 FN_API int fn_reset_energy(fn_ctx* ctx);
 
 /* Waits for the context's stream (OpenclManager::RunKernels). */
+/* Waits for the context's work.  Returns FN_ERR_NONFINITE once a step has
+   produced a NaN or infinite force (the state is then unusable). */
 FN_API int fn_sync(fn_ctx* ctx);
 
 /* Blocking read of one bead field, 3 doubles per bead, all networks in upload
@@ -313,6 +329,10 @@ FN_API int fn_forces_only(fn_ctx* ctx, int terms);
 
 /* Internal bead numbering: perm[internal] = upload index. */
 FN_API int fn_get_permutation(fn_ctx* ctx, int* perm);
+
+/* The device array of field (FN_POSITION, FN_IMAGE, FN_VELOCITY, FN_FORCE,
+   FN_VELOCITY_OLD) without a copy; synchronises the context's stream first. */
+FN_API int fn_device_view(fn_ctx* ctx, int field, fn_view* out);
 
 /* Times steps_per_trial steps at each candidate block size (64 .. 512) from
    one snapshot of the state, restored after every trial, and keeps the
