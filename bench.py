@@ -603,24 +603,36 @@ def run_adjoint(args):
                "median_rel_err_k_start": float(np.median(np.abs(k0 / true_k - 1))),
                "median_rel_err_k_fit": float(np.median(np.abs(k_fit / true_k - 1)))}
     curve.close()
+    from fibrenet_b200.ranks import slowest, total
+    # networks are independent: the loss and the bead count add up over the
+    # ranks, times are the slowest rank's, gradient norms combine as squares
+    t_plain, t_fwd, t_bwd = (slowest(t, dist, "cuda") for t in (t_plain, t_fwd, t_bwd))
+    loss0 = total(loss0, dist, "cuda")
+    nb_all = int(total(nb, dist, "cuda"))
+    gnorm = {k: float(np.sqrt(total(float(np.sum(np.asarray(v) ** 2)), dist, "cuda")))
+             for k, v in grads.items()}
+    if fit is not None:
+        fit["loss_first"] = total(fit["loss_first"], dist, "cuda")
+        fit["loss_last"] = total(fit["loss_last"], dist, "cuda")
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
-    line = {"metric": "adjoint/forward time (64-network tensile fit, 1 B200)",
+    line = {"metric": "adjoint/forward time (64-network tensile fit)",
             "value": t_bwd / t_plain, "unit": "ratio", "n_gpus": world, "steps": steps, "warmup": 1,
             "ms_per_step": t_bwd / steps, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 forces / f32 state / f64 gradient sums",
             "data": "synthetic (seeded generator; target from lognormal(0, 0.2) stiffness factors)",
-            "config": {"workload": f"fit_{len(all_ms)}", "networks": len(all_ms), "beads": nb,
+            "config": {"workload": f"fit_{len(all_ms)}", "networks": len(all_ms), "beads": nb_all,
                        "every": every, "checkpoint_every": ckpt, "loss": "sum (R_x - R*_x)^2",
                        "params": {"spring_k": len(k0), "spring_rest": len(r0), "angle_k": len(a0),
-                                  "pos0": 3 * nb}},
+                                  "pos0": 3 * nb, "per": "rank 0"},
+                       "parallelism": f"networks split over {world} rank(s) by bead count"},
             "forward_ms": t_plain, "recorded_forward_ms": t_fwd, "backward_ms": t_bwd,
-            "forward_bead_steps_per_s": nb * steps / (t_plain / 1e3),
+            "forward_bead_steps_per_s": nb_all * steps / (t_plain / 1e3),
             "backward_over_recorded_forward": t_bwd / t_fwd, "loss": loss0,
-            "grad_norm": {k: float(np.linalg.norm(v)) for k, v in grads.items()},
+            "grad_norm": gnorm,
             "fit": fit, "clocks": clk}
     print(json.dumps(line), flush=True)
 
