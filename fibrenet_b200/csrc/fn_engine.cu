@@ -155,6 +155,8 @@ void free_all(fn_ctx* c) {
     dfree(c, c->cell_start);
     dfree(c, c->cell_beads);
     dfree(c, c->ref_img);
+    dfree(c, c->inv_d);
+    dfree(c, c->export_xyz);
     dfree(c, c->gate);
     dfree(c, c->list_count);
     dfree(c, c->list);
@@ -285,21 +287,31 @@ void network_order(const fn_network_desc& d, const FnNet& N, bool reorder, std::
     order.resize(n);
     std::iota(order.begin(), order.end(), 0);
     if (!reorder || n == 0) return;
-    std::vector<int> parent(n);
-    std::iota(parent.begin(), parent.end(), 0);
-    auto find = [&](int x) {
-        while (parent[x] != x) {
-            parent[x] = parent[parent[x]];
-            x = parent[x];
-        }
-        return x;
-    };
-    for (int s = 0; s < d.n_springs; ++s) {
-        int a = find(d.s_p1[s]), b = find(d.s_p2[s]);
-        if (a != b) parent[std::max(a, b)] = std::min(a, b);
-    }
     std::vector<int> root(n);
-    for (int i = 0; i < n; ++i) root[i] = find(i);
+    /* fibres listed bead after bead (every spring joins i and i + 1): each
+       component is a run of consecutive beads, labelled by one sweep */
+    bool runs = true;
+    for (int s = 0; s < d.n_springs && runs; ++s) runs = std::abs(d.s_p1[s] - d.s_p2[s]) == 1;
+    if (runs) {
+        std::vector<unsigned char> link(n, 0); /* spring between i and i + 1 */
+        for (int s = 0; s < d.n_springs; ++s) link[std::min(d.s_p1[s], d.s_p2[s])] = 1;
+        for (int i = 0; i < n; ++i) root[i] = (i > 0 && link[i - 1]) ? root[i - 1] : i;
+    } else {
+        std::vector<int> parent(n);
+        std::iota(parent.begin(), parent.end(), 0);
+        auto find = [&](int x) {
+            while (parent[x] != x) {
+                parent[x] = parent[parent[x]];
+                x = parent[x];
+            }
+            return x;
+        };
+        for (int s = 0; s < d.n_springs; ++s) {
+            int a = find(d.s_p1[s]), b = find(d.s_p2[s]);
+            if (a != b) parent[std::max(a, b)] = std::min(a, b);
+        }
+        for (int i = 0; i < n; ++i) root[i] = find(i);
+    }
     /* components (roots = their lowest bead) sorted by the Morton code of
        their first bead, ties by index; then every component's beads in
        ascending order: a stable sort of the beads by (key of root, index)
@@ -959,6 +971,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     /* bead order */
     c->perm.assign(nb, 0);
     c->inv.assign(nb, 0);
+    dfree(c, c->inv_d); /* the export's copy of the numbering, rebuilt on first use */
     for (int k = 0; k < n_networks; ++k) {
         std::vector<int> order;
         network_order(nets[k], c->nets_h[k], c->cfg.reorder != 0, order);
@@ -1185,33 +1198,26 @@ FN_API int fn_download(fn_ctx* c, int field, double* host) {
     if (!host) return fail(c, FN_ERR_ARG, "fn_download: null host pointer");
     CK(cudaSetDevice(c->cfg.device));
     const long long nb = c->nb;
+    /* permuted and unpacked on the device, then one copy into the caller's
+       x, y, z layout */
+    if (!c->inv_d.p || c->export_xyz.n < (size_t)(3 * nb)) {
+        CK(dalloc(c, c->inv_d, (size_t)nb));
+        CK(dalloc(c, c->export_xyz, (size_t)(3 * nb)));
+        CK(h2d(c, c->inv_d, c->inv));
+    }
     if (field == FN_POSITION || field == FN_IMAGE) {
-        std::vector<double4> tmp(nb);
         const DevBuf<double4>& b = field == FN_POSITION ? c->pos[c->cur] : c->img[c->cur];
-        CK(cudaMemcpyAsync(tmp.data(), b.p, sizeof(double4) * nb, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        for (long long q = 0; q < nb; ++q) {
-            const long long i = c->perm[q];
-            host[3 * i] = tmp[q].x;
-            host[3 * i + 1] = tmp[q].y;
-            host[3 * i + 2] = tmp[q].z;
-        }
-        return FN_OK;
+        CK(fn::launch_export_xyz(b.p, c->inv_d.p, (int)nb, c->export_xyz.p, c->stream));
+    } else {
+        const DevBuf<float4>* b = field == FN_VELOCITY ? &c->vel
+                                  : field == FN_FORCE  ? &c->force
+                                  : field == FN_VELOCITY_OLD ? &c->vold
+                                                             : nullptr;
+        if (!b) return fail(c, FN_ERR_ARG, "fn_download: unknown field");
+        CK(fn::launch_export_xyz(b->p, c->inv_d.p, (int)nb, c->export_xyz.p, c->stream));
     }
-    const DevBuf<float4>* b = field == FN_VELOCITY ? &c->vel
-                              : field == FN_FORCE  ? &c->force
-                              : field == FN_VELOCITY_OLD ? &c->vold
-                                                         : nullptr;
-    if (!b) return fail(c, FN_ERR_ARG, "fn_download: unknown field");
-    std::vector<float4> tmp(nb);
-    CK(cudaMemcpyAsync(tmp.data(), b->p, sizeof(float4) * nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(host, c->export_xyz.p, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    for (long long q = 0; q < nb; ++q) {
-        const long long i = c->perm[q];
-        host[3 * i] = tmp[q].x;
-        host[3 * i + 1] = tmp[q].y;
-        host[3 * i + 2] = tmp[q].z;
-    }
     return FN_OK;
 }
 

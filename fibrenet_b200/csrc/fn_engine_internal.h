@@ -119,6 +119,10 @@ struct fn_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_step, ev_rebuild;
     size_t ev_next = 0;
 
+    /* export: upload -> internal bead index on the device, x/y/z staging */
+    DevBuf<int> inv_d;
+    DevBuf<double> export_xyz;
+
     /* displacement-triggered rebuilds (cfg.verlet_skin > 0) */
     bool verlet = false;
     double verlet_thresh2 = 0.0; /* squared bead displacement that forces a rebuild */

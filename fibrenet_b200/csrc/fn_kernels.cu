@@ -1421,6 +1421,29 @@ cudaError_t launch_verlet_rebuild(const RebuildArgs& R, const FnTile* tiles, con
     return cudaGetLastError();
 }
 
+/* Export of one bead field in upload order as x, y, z doubles (the host
+   buffer layout of fn_download): out[3 u + a] = src[inv[u]].a. */
+template <class T>
+__global__ void k_export_xyz(const T* __restrict__ src, const int* __restrict__ inv, int n,
+                             double* __restrict__ out) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    const T v = src[inv[u]];
+    out[3 * (size_t)u] = (double)v.x;
+    out[3 * (size_t)u + 1] = (double)v.y;
+    out[3 * (size_t)u + 2] = (double)v.z;
+}
+
+cudaError_t launch_export_xyz(const double4* src, const int* inv, int n, double* out, cudaStream_t s) {
+    if (n > 0) k_export_xyz<double4><<<(n + 255) / 256, 256, 0, s>>>(src, inv, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export_xyz(const float4* src, const int* inv, int n, double* out, cudaStream_t s) {
+    if (n > 0) k_export_xyz<float4><<<(n + 255) / 256, 256, 0, s>>>(src, inv, n, out);
+    return cudaGetLastError();
+}
+
 /* ---------------------------------------------------------------------------
    Energy and virial (an addition: the reference computes neither).  Each term
    is the potential whose negative gradient is the force the step applies:

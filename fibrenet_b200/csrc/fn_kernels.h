@@ -189,6 +189,9 @@ struct EnergyArgs {
 };
 
 cudaError_t launch_energy(const EnergyArgs& E, int nblocks, double* out, cudaStream_t s);
+/* one bead field in upload order as x, y, z doubles (inv: upload -> internal) */
+cudaError_t launch_export_xyz(const double4* src, const int* inv, int n, double* out, cudaStream_t s);
+cudaError_t launch_export_xyz(const float4* src, const int* inv, int n, double* out, cudaStream_t s);
 
 cudaError_t launch_step(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
                         bool store_v, cudaStream_t s);
