@@ -254,10 +254,8 @@ FO_EXPORT fo_ctx* fo_create(const fo_model* m, int mode, int cell_cap, int list_
         c->p_kind[p] = m->pair_kind[p];
         fo_derive_pair(m->pair_kind[p], m->pair_raw + 4 * p, c->p_c + 6 * p);
     }
-    fo_derived dd = c->d;
-    dd.bc_type = (c->periodic == 7) ? 0 : 1;
     c->cell_nh = (int*)zal(sizeof(int) * 13 * (size_t)c->d.ncells);
-    fo_cell_neighbours(&dd, c->cell_nh);
+    fo_cell_neighbours_mask(&c->d, c->periodic, c->cell_nh);
     c->grid_head = (int*)zal(sizeof(int) * (size_t)c->d.ncells);
     c->grid_slot = (int*)zal(sizeof(int) * (size_t)c->d.ncells * (size_t)c->cell_cap);
     c->bead_cell = (int*)zal(ni);

@@ -124,6 +124,20 @@ static inline int fo_nh_cell(const fo_derived* d, int nx, int ny, int nz) {
     return nx + ny * d->nx + nz * d->nx * d->ny;
 }
 
+/* The same decision per axis for a box periodic on the axes of mask and
+   finite on the others (the per-axis boundary extension; mask 7 gives the
+   pbc table above, 0 the finite one). */
+static inline int fo_nh_cell_mask(const fo_derived* d, int mask, int nx, int ny, int nz) {
+    int q[3] = {nx, ny, nz};
+    const int n[3] = {d->nx, d->ny, d->nz};
+    for (int a = 0; a < 3; ++a) {
+        if (q[a] >= 0 && q[a] < n[a]) continue;
+        if (!((mask >> a) & 1)) return -1;
+        q[a] = q[a] < 0 ? n[a] - 1 : 0;
+    }
+    return q[0] + q[1] * d->nx + q[2] * d->nx * d->ny;
+}
+
 /* The 13-cell half-shell table, SimulationManager.cpp:2210-2301: nine cells
    at z-1 (dx outer, dy inner), three at x+1 (dy = -1..1), one at y-1. */
 static inline void fo_cell_neighbours(const fo_derived* d, int* nh) {
@@ -137,6 +151,21 @@ static inline void fo_cell_neighbours(const fo_derived* d, int* nh) {
                     for (int dy = -1; dy < 2; dy++) row[cnt++] = fo_nh_cell(d, xx + dx, yy + dy, zz - 1);
                 for (int dy = -1; dy < 2; dy++) row[cnt++] = fo_nh_cell(d, xx + 1, yy + dy, zz);
                 row[cnt++] = fo_nh_cell(d, xx, yy - 1, zz);
+            }
+}
+
+/* The half-shell table of a box periodic on the axes of mask. */
+static inline void fo_cell_neighbours_mask(const fo_derived* d, int mask, int* nh) {
+    for (int zz = 0; zz < d->nz; zz++)
+        for (int yy = 0; yy < d->ny; yy++)
+            for (int xx = 0; xx < d->nx; xx++) {
+                int target = xx + yy * d->nx + zz * d->nx * d->ny;
+                int* row = nh + (long)target * 13;
+                int cnt = 0;
+                for (int dx = -1; dx < 2; dx++)
+                    for (int dy = -1; dy < 2; dy++) row[cnt++] = fo_nh_cell_mask(d, mask, xx + dx, yy + dy, zz - 1);
+                for (int dy = -1; dy < 2; dy++) row[cnt++] = fo_nh_cell_mask(d, mask, xx + 1, yy + dy, zz);
+                row[cnt++] = fo_nh_cell_mask(d, mask, xx, yy - 1, zz);
             }
 }
 
