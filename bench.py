@@ -374,7 +374,15 @@ def run_ours(args):
     # observables read back after each chunk, final state download
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, m, local, dist, world, nb, barrier)
+        # three end-to-end runs, the median reported: host-side allocation
+        # and page-mapping times on these shared machines vary from run to
+        # run by up to a few hundred ms
+        runs = [run_e2e(args, m, local, dist, world, nb, barrier) for _ in range(3)]
+        vals = sorted(r["value"] for r in runs)
+        e2e = dict(runs[0])
+        e2e["value"] = vals[1]
+        e2e["runs"] = [r["value"] for r in runs]
+        e2e["what"] = runs[0]["what"] + " (median of 3 runs)"
 
     peak, peak_kind = peaks()
     alg = algorithmic_bytes(m, half_pairs)

@@ -444,35 +444,67 @@ bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<
     using namespace fn;
     const long long nb = c->nb;
     std::vector<int> next_sp(nb, -1), centre_an(nb, -1);
-    std::vector<unsigned char> fl(nb, 0);
-    for (long long s = 0; s < c->ns; ++s) {
-        const int a = sp_ends[s].x, b = sp_ends[s].y;
-        const int lo = std::min(a, b), hi = std::max(a, b);
-        if (hi != lo + 1 || next_sp[lo] != -1) return false;
-        next_sp[lo] = (int)s;
-        fl[lo] |= FN_CH_SPRING;
-        if (a == hi) fl[lo] |= FN_CH_SP_REV;
-        if (sp_type[s] == 1)
-            fl[lo] |= FN_CH_SP_FL;
-        else if (sp_type[s] != 0)
-            fl[lo] |= FN_CH_SP_INERT;
-    }
-    for (long long a = 0; a < c->na; ++a) {
-        const int4 b = an_b[a];
-        const bool fwd = b.x == b.y - 1 && b.z == b.y + 1;
-        const bool rev = b.x == b.y + 1 && b.z == b.y - 1;
-        if (!(fwd || rev) || centre_an[b.y] != -1) return false;
-        centre_an[b.y] = (int)a;
-        fl[b.y] |= FN_CH_ANGLE;
-        if (rev) fl[b.y] |= FN_CH_AN_REV;
-        if (b.w == 1) {
-            fl[b.y] |= FN_CH_AN_FL;
-            const int sp = next_sp[b.y - 1], sn = next_sp[b.y];
-            const int2 ss = an_s[a];
-            if (sp < 0 || sn < 0) return false;
-            if (!((ss.x == sp && ss.y == sn) || (ss.x == sn && ss.y == sp))) return false;
+    std::vector<unsigned char> fl(nb, 0), fa(nb, 0);
+    std::atomic<bool> bad_form{false};
+    /* springs, then angles, each on host threads: in chain form every lower
+       bead has at most one spring and every centre at most one angle, so the
+       writes do not collide; a second sweep catches the models where they
+       would (two bonds claiming one slot) */
+    parallel_for(c->ns, [&](long long s0, long long s1) {
+        for (long long s = s0; s < s1; ++s) {
+            const int a = sp_ends[s].x, b = sp_ends[s].y;
+            const int lo = std::min(a, b), hi = std::max(a, b);
+            if (hi != lo + 1) {
+                bad_form = true;
+                continue;
+            }
+            next_sp[lo] = (int)s;
+            unsigned char f = FN_CH_SPRING;
+            if (a == hi) f |= FN_CH_SP_REV;
+            if (sp_type[s] == 1)
+                f |= FN_CH_SP_FL;
+            else if (sp_type[s] != 0)
+                f |= FN_CH_SP_INERT;
+            fl[lo] = f;
         }
-    }
+    });
+    if (bad_form) return false;
+    parallel_for(c->ns, [&](long long s0, long long s1) {
+        for (long long s = s0; s < s1; ++s)
+            if (next_sp[std::min(sp_ends[s].x, sp_ends[s].y)] != (int)s) bad_form = true;
+    });
+    if (bad_form) return false;
+    parallel_for(c->na, [&](long long a0, long long a1) {
+        for (long long a = a0; a < a1; ++a) {
+            const int4 b = an_b[a];
+            const bool fwd = b.x == b.y - 1 && b.z == b.y + 1;
+            const bool rev = b.x == b.y + 1 && b.z == b.y - 1;
+            if (!(fwd || rev)) {
+                bad_form = true;
+                continue;
+            }
+            centre_an[b.y] = (int)a;
+            unsigned char f = FN_CH_ANGLE;
+            if (rev) f |= FN_CH_AN_REV;
+            if (b.w == 1) {
+                f |= FN_CH_AN_FL;
+                const int sp = next_sp[b.y - 1], sn = next_sp[b.y];
+                const int2 ss = an_s[a];
+                if (sp < 0 || sn < 0 || !((ss.x == sp && ss.y == sn) || (ss.x == sn && ss.y == sp)))
+                    bad_form = true;
+            }
+            fa[b.y] = f;
+        }
+    });
+    if (bad_form) return false;
+    parallel_for(c->na, [&](long long a0, long long a1) {
+        for (long long a = a0; a < a1; ++a)
+            if (centre_an[an_b[a].y] != (int)a) bad_form = true;
+    });
+    if (bad_form) return false;
+    parallel_for(nb, [&](long long i0, long long i1) {
+        for (long long i = i0; i < i1; ++i) fl[i] |= fa[i];
+    });
     std::atomic<bool> bad{false};
     parallel_for(nb, [&](long long i0, long long i1) {
         for (long long i = i0; i < i1; ++i) {
@@ -966,6 +998,55 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     c->ns = ns;
     c->na = na;
     c->ncells = ncells;
+    c->list_stride = (int)((nb + 31) / 32 * 32);
+    /* device allocations on a helper thread while this one orders and
+       converts the model (the sizes are known from here on) */
+    cudaError_t alloc_err = cudaSuccess;
+    std::string alloc_what;
+    std::thread allocator([&, nb, ns, na, ncells, n_networks] {
+        if ((alloc_err = cudaSetDevice(c->cfg.device)) != cudaSuccess) return;
+#define AL(call)                          \
+    do {                                  \
+        if ((alloc_err = (call)) != cudaSuccess) { \
+            alloc_what = #call;           \
+            return;                       \
+        }                                 \
+    } while (0)
+    const size_t list_n = (size_t)c->list_stride * (size_t)c->cfg.list_capacity;
+        for (int k = 0; k < 2; ++k) {
+            AL(dalloc(c, c->pos[k], nb));
+            AL(dalloc(c, c->img[k], nb));
+        }
+        AL(dalloc(c, c->vold, nb));
+        AL(dalloc(c, c->force, nb));
+        AL(dalloc(c, c->vel, nb));
+        AL(dalloc(c, c->binfo, nb));
+        AL(dalloc(c, c->sp_ends, ns));
+        AL(dalloc(c, c->sp_par, ns));
+        AL(dalloc(c, c->sp_type, ns));
+        AL(dalloc(c, c->sp_status, ns));
+        AL(dalloc(c, c->an_b, na));
+        AL(dalloc(c, c->an_s, na));
+        AL(dalloc(c, c->an_par, na));
+        AL(dalloc(c, c->an_status, na));
+        AL(dalloc(c, c->cell_of, nb));
+        AL(dalloc(c, c->cell_count, ncells));
+        AL(dalloc(c, c->cell_fill, ncells));
+        AL(dalloc(c, c->cell_start, ncells + 1));
+        AL(dalloc(c, c->cell_beads, nb));
+        AL(dalloc(c, c->list_count, nb));
+        AL(dalloc(c, c->list, list_n));
+        AL(dalloc(c, c->scan_sums, (size_t)fn::scan_block_count(ncells) + 1));
+        AL(dalloc(c, c->nets, n_networks));
+        AL(dalloc(c, c->pairs, c->pairs_h.size()));
+        AL(dalloc(c, c->counters, FN_CNT_N));
+        AL(dalloc(c, c->obs_partial, 5 * 1024));
+        AL(dalloc(c, c->obs_out, 8));
+        AL(dalloc(c, c->en_partial, (size_t)fn::FN_EN_N * 1024));
+        AL(dalloc(c, c->en_out, fn::FN_EN_N));
+#undef AL
+    });
+
     c->grid_update_freq = c->info[0].grid_update_freq;
 
     /* bead order */
@@ -1048,64 +1129,51 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     c->incidence_ready = false;
     c->an_b_h = an_b;
     c->an_s_h = an_s;
-    c->list_stride = (int)((nb + 31) / 32 * 32);
-    const size_t list_n = (size_t)c->list_stride * (size_t)c->cfg.list_capacity;
-    for (int k = 0; k < 2; ++k) {
-        CK(dalloc(c, c->pos[k], nb));
-        CK(dalloc(c, c->img[k], nb));
-    }
-    CK(dalloc(c, c->vold, nb));
-    CK(dalloc(c, c->force, nb));
-    CK(dalloc(c, c->vel, nb));
-    CK(dalloc(c, c->binfo, nb));
-    CK(dalloc(c, c->sp_ends, ns));
-    CK(dalloc(c, c->sp_par, ns));
-    CK(dalloc(c, c->sp_type, ns));
-    CK(dalloc(c, c->sp_status, ns));
-    CK(dalloc(c, c->an_b, na));
-    CK(dalloc(c, c->an_s, na));
-    CK(dalloc(c, c->an_par, na));
-    CK(dalloc(c, c->an_status, na));
-    CK(dalloc(c, c->cell_of, nb));
-    CK(dalloc(c, c->cell_count, ncells));
-    CK(dalloc(c, c->cell_fill, ncells));
-    CK(dalloc(c, c->cell_start, ncells + 1));
-    CK(dalloc(c, c->cell_beads, nb));
-    CK(dalloc(c, c->list_count, nb));
-    CK(dalloc(c, c->list, list_n));
-    CK(dalloc(c, c->scan_sums, (size_t)fn::scan_block_count(ncells) + 1));
-    CK(dalloc(c, c->nets, n_networks));
-    CK(dalloc(c, c->pairs, c->pairs_h.size()));
-    CK(dalloc(c, c->counters, FN_CNT_N));
-    CK(dalloc(c, c->obs_partial, 5 * 1024));
-    CK(dalloc(c, c->obs_out, 8));
-    CK(dalloc(c, c->en_partial, (size_t)fn::FN_EN_N * 1024));
-    CK(dalloc(c, c->en_out, fn::FN_EN_N));
-
+    allocator.join();
+    if (alloc_err != cudaSuccess)
+        return fail(c, alloc_err == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA,
+                    alloc_what + ": " + cudaGetErrorString(alloc_err));
     c->cur = 0;
-    CK(h2d(c, c->pos[0], pos));
-    CK(h2d(c, c->img[0], img));
-    CK(cudaMemcpyAsync(c->pos[1].p, c->pos[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->img[1].p, c->img[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
-    CK(h2d(c, c->vold, vold));
-    CK(h2d(c, c->force, force));
-    CK(h2d(c, c->vel, vel));
-    CK(h2d(c, c->binfo, binfo));
-    CK(h2d(c, c->sp_ends, sp_ends));
-    CK(h2d(c, c->sp_par, c->sp_par_h));
-    CK(h2d(c, c->sp_type, sp_type));
-    CK(h2d(c, c->sp_status, sp_status));
-    CK(h2d(c, c->an_b, an_b));
-    CK(h2d(c, c->an_s, an_s));
-    CK(h2d(c, c->an_par, c->an_par_h));
-    CK(h2d(c, c->an_status, an_status));
-    CK(h2d(c, c->nets, c->nets_h));
-    CK(h2d(c, c->pairs, c->pairs_h));
-    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * FN_CNT_N, c->stream));
-    CK(cudaMemsetAsync(c->list_count.p, 0, sizeof(int) * (size_t)nb, c->stream));
-    CK(cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
-    CK(cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
+    /* host-to-device copies on a helper thread while this one builds the
+       chain records */
+    cudaError_t copy_err = cudaSuccess;
+    std::string copy_what;
+    std::thread copier([&] {
+        if ((copy_err = cudaSetDevice(c->cfg.device)) != cudaSuccess) return;
+#define CP(call)                          \
+    do {                                  \
+        if ((copy_err = (call)) != cudaSuccess) { \
+            copy_what = #call;            \
+            return;                       \
+        }                                 \
+    } while (0)
+        CP(h2d(c, c->pos[0], pos));
+        CP(h2d(c, c->img[0], img));
+        CP(cudaMemcpyAsync(c->pos[1].p, c->pos[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
+        CP(cudaMemcpyAsync(c->img[1].p, c->img[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
+        CP(h2d(c, c->vold, vold));
+        CP(h2d(c, c->force, force));
+        CP(h2d(c, c->vel, vel));
+        CP(h2d(c, c->binfo, binfo));
+        CP(h2d(c, c->sp_ends, sp_ends));
+        CP(h2d(c, c->sp_par, c->sp_par_h));
+        CP(h2d(c, c->sp_type, sp_type));
+        CP(h2d(c, c->sp_status, sp_status));
+        CP(h2d(c, c->an_b, an_b));
+        CP(h2d(c, c->an_s, an_s));
+        CP(h2d(c, c->an_par, c->an_par_h));
+        CP(h2d(c, c->an_status, an_status));
+        CP(h2d(c, c->nets, c->nets_h));
+        CP(h2d(c, c->pairs, c->pairs_h));
+        CP(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * FN_CNT_N, c->stream));
+        CP(cudaMemsetAsync(c->list_count.p, 0, sizeof(int) * (size_t)nb, c->stream));
+        CP(cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
+        CP(cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
+#undef CP
+    });
     c->chain = c->cfg.chain_mode != 2 && build_chain(c, sp_ends, sp_type, an_b, an_s);
+    copier.join();
+    if (copy_err != cudaSuccess) return fail(c, FN_ERR_CUDA, copy_what + ": " + cudaGetErrorString(copy_err));
     int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128);
     if (r) return r;
     r = verlet_setup(c);
