@@ -47,11 +47,14 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
-    p.add_argument("--workload", choices=["tensile", "dense", "ensemble", "adjoint"], default="tensile",
+    p.add_argument("--workload", choices=["tensile", "dense", "ensemble", "adjoint", "plain"],
+                   default="tensile",
                    help="tensile: the 1M-bead network (default, the headline); dense: the 4M-bead "
                         "periodic 3D mat with penalty + soft-repulsion contacts; ensemble: 256 "
                         "independent networks batched in one context vs run one by one; adjoint: "
-                        "64 networks, reaction-curve loss, forward + backward sweep vs forward")
+                        "64 networks, reaction-curve loss, forward + backward sweep vs forward; plain: "
+                        "the 10k-bead network of the reference's CPU-runnable case, us per step "
+                        "with the steps replayed as CUDA graphs")
     p.add_argument("--networks", type=int, default=None)
     p.add_argument("--adam-iters", type=int, default=0,
                    help="adjoint workload: stiffness-recovery iterations after the timing")
@@ -645,6 +648,67 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def run_plain(args):
+    """The small network (200 fibres x 50 beads, penalty contacts): its working
+    set sits in L2, so the step is launch- and latency-bound; steps run as
+    CUDA graphs, timed with CUDA events, then the kernels alone with timing."""
+    import torch
+
+    from fibrenet_b200 import generate as g
+    from fibrenet_b200.native import Simulation
+    from fibrenet_b200.ranks import job_rate, slowest
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    m = g.plain_network(seed=0)
+    sim = Simulation(m, device=local, list_capacity=64, reorder=True, use_graphs=True)
+    sim.step(max(args.warmup, 3))
+    sim.sync()
+    K = args.steps
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0.record()
+    sim.step(K)
+    sim.sync()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    sim.enable_timing(True)
+    sim.step(min(K, 400))
+    kt = sim.kernel_time()
+    sim.close()
+    value = job_rate(m.n_beads * K, ms, dist, "cuda")
+    ms = slowest(ms, dist, "cuda")
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": "bead-steps/s (10k-bead network, steps as CUDA graphs)", "value": value,
+            "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms / K, "us_per_step": 1e3 * ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": "plain_10k", "beads": m.n_beads, "fibres": 200, "beads_per_fibre": 50,
+                       "box": list(m.settings.box), "contacts": "penalty k 50", "dt": m.settings.dt,
+                       "grid_update_freq": m.settings.grid_update_freq, "graphs": True,
+                       "l2": "working set in L2 (launch- and latency-bound, not judged against HBM)"},
+            "step_kernel_us": 1e3 * kt["step_ms"], "rebuild_us": 1e3 * kt["rebuild_ms"], "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -653,6 +717,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "plain":
+        run_plain(args)
     else:
         run_ours(args)
 
