@@ -68,6 +68,8 @@ def parse():
 
 def workload(args):
     from fibrenet_b200 import generate as g
+    if args.workload == "plain":
+        return g.plain_network(seed=0)
     if args.workload == "dense":
         s = (args.fibres / 40000.0) ** (1.0 / 3.0)
         return g.dense_mat(seed=2, fibres=args.fibres, beads=100, box=(200.0 * s,) * 3)
@@ -78,12 +80,21 @@ def workload(args):
 
 
 def metric_for(args):
+    if args.workload == "plain":
+        return "bead-steps/s (10k-bead network, steps as CUDA graphs)"
     if args.workload == "dense":
         return "bead-steps/s (dense 3D mat, 1 B200 per replica)"
     return METRIC
 
 
 def config_dict(m, args, extra=None):
+    if args.workload == "plain":
+        d = {"workload": "plain_10k", "beads": m.n_beads, "fibres": 200, "beads_per_fibre": 50,
+             "box": list(m.settings.box), "contacts": "penalty k 50", "dt": m.settings.dt,
+             "grid_update_freq": m.settings.grid_update_freq}
+        if extra:
+            d.update(extra)
+        return d
     if args.workload == "dense":
         name = "dense_4M" if args.fibres == 40000 else f"dense_{m.n_beads}"
         d = {"workload": name, "beads": m.n_beads, "springs": m.n_springs, "angles": m.n_angles,
@@ -240,6 +251,16 @@ def cpu_reference_rate(model, seconds: float, threads: int | None = None, steps_
     return m.n_beads * done / dt, done, threads, kind
 
 
+def ref_note(args) -> dict:
+    """What the reference's kernels run instead where they cannot express the
+    workload exactly."""
+    if args.workload == "tensile":
+        return {"boundary_in_reference": "walls on all axes"}
+    if args.workload == "dense":
+        return {"contacts_in_reference": "hs penalty k 100 only (one pair kind per type pair in the reference)"}
+    return {}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -252,10 +273,7 @@ def run_reference_arm(args):
             "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * m.n_beads / rate,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator)", "impl": "reference",
-            "config": config_dict(m, args, {"boundary_in_reference": "walls on all axes"}
-                                  if args.workload == "tensile" else
-                                  {"contacts_in_reference": "hs penalty k 100 only (one pair kind "
-                                                            "per type pair in the reference)"}),
+            "config": config_dict(m, args, ref_note(args)),
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": f"{done} whole steps of the full {m.n_beads}-bead network "
                                        f"(time-bounded, {budget:.0f} s)"},
@@ -398,8 +416,7 @@ def run_ours(args):
         rate, done_cpu, threads, kind = cpu_reference_rate(m, args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{done_cpu} whole steps of the same {nb}-bead network on the host "
-                         f"(reference kernels as C, OpenMP, "
-                         f"{'walls on all axes' if args.workload == 'tensile' else 'hs penalty only'})"}
+                         f"(reference kernels as C, OpenMP{''.join(', ' + v for v in ref_note(args).values())})"}
 
     if rank == 0:
         line = {
@@ -701,10 +718,8 @@ def run_plain(args):
             "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(args.warmup, 3),
             "ms_per_step": ms / K, "us_per_step": 1e3 * ms / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": "plain_10k", "beads": m.n_beads, "fibres": 200, "beads_per_fibre": 50,
-                       "box": list(m.settings.box), "contacts": "penalty k 50", "dt": m.settings.dt,
-                       "grid_update_freq": m.settings.grid_update_freq, "graphs": True,
-                       "l2": "working set in L2 (launch- and latency-bound, not judged against HBM)"},
+            "config": config_dict(m, args, {"graphs": True, "l2": "working set in L2 (launch- and "
+                                            "latency-bound, not judged against HBM)"}),
             "step_kernel_us": 1e3 * kt["step_ms"], "rebuild_us": 1e3 * kt["rebuild_ms"], "clocks": clk}
     print(json.dumps(line), flush=True)
 
