@@ -613,7 +613,10 @@ int set_block(fn_ctx* c, int block) {
                                        std::to_string(fn::kChainMaxBlock) + " threads per block");
     drop_graphs(c);
     std::vector<FnTile> t;
-    int n = build_tiles(c, block, t);
+    /* the chain kernel stages its tile plus a two-bead halo on each side:
+       tiles of block - 4 beads make that exactly one slot per thread, so no
+       warp runs a second round of the spring and angle phases */
+    int n = build_tiles(c, c->chain ? block - 4 : block, t);
     CK(cudaStreamSynchronize(c->stream));
     CK(dalloc(c, c->tiles, t.size()));
     CK(h2d(c, c->tiles, t));
