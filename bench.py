@@ -281,7 +281,7 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(args, m, local, dist, world, nb, barrier):
+def run_e2e(args, m, local, dist, world, nb, barrier, block=0):
     """Same metric through the public API with host buffers: model upload from
     pinned host arrays, RunSimulationLoop in output_freq chunks with the
     recorded observables read back after each chunk, final state download."""
@@ -301,7 +301,8 @@ def run_e2e(args, m, local, dist, world, nb, barrier):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     w0 = time.perf_counter()
-    sim2 = Simulation(mm, device=local, list_capacity=64, cell_capacity=64, reorder=True)
+    sim2 = Simulation(mm, device=local, list_capacity=64, cell_capacity=64, reorder=True,
+                      block_size=block)
     done = 0
     obs_bytes = 0
     while done < e2e_steps:
@@ -356,6 +357,8 @@ def run_ours(args):
     nb = m.n_beads
 
     sim.step(max(args.warmup, 3))
+    block = sim.autotune(16)  # block size of the step kernel; the state is restored
+    sim.step(8)
     sim.sync()
     sim.rebuild()
     cnt, _ = sim.lists()
@@ -398,7 +401,7 @@ def run_ours(args):
         # three end-to-end runs, the median reported: host-side allocation
         # and page-mapping times on these shared machines vary from run to
         # run by up to a few hundred ms
-        runs = [run_e2e(args, m, local, dist, world, nb, barrier) for _ in range(3)]
+        runs = [run_e2e(args, m, local, dist, world, nb, barrier, block) for _ in range(3)]
         vals = sorted(r["value"] for r in runs)
         e2e = dict(runs[0])
         e2e["value"] = vals[1]
@@ -424,7 +427,7 @@ def run_ours(args):
             "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator; reference ships no models)",
-            "config": config_dict(m, args, {"half_list_pairs": half_pairs,
+            "config": config_dict(m, args, {"half_list_pairs": half_pairs, "block_size": block,
                                             "storage": "positions f64, velocities/forces f32"}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
