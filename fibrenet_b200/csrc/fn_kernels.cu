@@ -710,12 +710,13 @@ __global__ void __launch_bounds__(kChainMaxBlock, 5) k_step_chain(const StepArgs
         }
     }
 
-    /* contacts, load-balanced inside each warp: the warp's beads' list items
-       are taken 32 at a time, lane l evaluating item (window base + l); a
-       32-byte map tells each lane whose item it holds, results go to shared
-       memory and every bead then adds its own items in list order (the order
-       of a sequential loop over its list, so the sums are identical).  Only
-       warp barriers are involved. */
+    /* contacts, load-balanced inside each warp: after a direct phase over the
+       leading items of every list, the remaining items are taken 32 at a
+       time, lane l evaluating item (window base + l); a 32-byte map tells each
+       lane whose item it holds, results go to shared memory and every bead
+       then adds its own items in list order (the order of a sequential loop
+       over its list, so the sums are identical).  Only warp barriers are
+       involved. */
     {
         const int lane = tid & 31, wid = tid >> 5;
         unsigned char* s_map = smem_raw + L.wmap + 32 * (size_t)wid;
@@ -724,22 +725,41 @@ __global__ void __launch_bounds__(kChainMaxBlock, 5) k_step_chain(const StepArgs
         const double4* s_pos = reinterpret_cast<const double4*>(smem_raw + L.pos);
         double4* s_pos_w = reinterpret_cast<double4*>(smem_raw + L.pos);
         if (active) s_pos_w[tid] = p;
-        int off = nc;
+        /* direct phase: every lane first evaluates the leading KD items of its
+           own list, one list row per iteration (coalesced loads, no window
+           bookkeeping); KD is the warp's mean list length rounded down, so
+           most lanes are busy in it and only the longer lists' tails go
+           through the windows */
+        const int kd = __reduce_add_sync(0xffffffffu, nc) >> 5;
+        const int nd = min(nc, kd);
+        for (int k = 0; k < kd; ++k) {
+            if (k < nd) {
+                const int j = A.list[(size_t)k * A.list_stride + i];
+                double Rx = 0.0, Ry = 0.0, Rz = 0.0;
+                if (contact_eval(N, A.pairs, p, A.pos_in[j], Rx, Ry, Rz)) {
+                    Fx += Rx;
+                    Fy += Ry;
+                    Fz += Rz;
+                }
+            }
+        }
+        const int nr = nc - nd; /* items left for the windows */
+        int off = nr;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, off, o);
             if (lane >= o) off += y;
         }
         const int total = __shfl_sync(0xffffffffu, off, 31);
-        off -= nc; /* exclusive */
+        off -= nr; /* exclusive */
         __syncwarp();
         for (int base = 0; base < total; base += 32) {
             const int lim = min(base + 32, total);
-            for (int w = max(off, base); w < min(off + nc, lim); ++w) s_map[w - base] = (unsigned char)lane;
+            for (int w = max(off, base); w < min(off + nr, lim); ++w) s_map[w - base] = (unsigned char)lane;
             __syncwarp();
             const int w = base + lane;
             const int b = w < lim ? s_map[lane] : 0;
-            const int ob = __shfl_sync(0xffffffffu, off, b);
+            const int ob = __shfl_sync(0xffffffffu, off - nd, b); /* list row = w - ob */
             if (w < lim) {
                 const int ib = (tid & ~31) + b; /* block-local bead of the item */
                 const int j = A.list[(size_t)(w - ob) * A.list_stride + (b0 + ib)];
@@ -751,7 +771,7 @@ __global__ void __launch_bounds__(kChainMaxBlock, 5) k_step_chain(const StepArgs
                 s_Rf[lane] = (unsigned char)acts;
             }
             __syncwarp();
-            for (int q = max(off, base); q < min(off + nc, lim); ++q) {
+            for (int q = max(off, base); q < min(off + nr, lim); ++q) {
                 if (s_Rf[q - base]) {
                     Fx += s_R[3 * (q - base)];
                     Fy += s_R[3 * (q - base) + 1];
