@@ -558,12 +558,12 @@ __device__ __forceinline__ int block_scan_any(int v, int* warp_sums, int& total)
    thread.  FORCES_ONLY evaluates the selected terms alone (no base force, no
    kick or drift, no status change). */
 template <bool DAMP, bool DRIFT, bool STORE_V, bool FORCES_ONLY>
-/* At most 256 threads per block and 5 such blocks per SM, i.e. at most 48
-   registers (a few spilled): the kernel waits on dependent loads of contact
-   partners, and the extra resident warps pay (measured on the 1M-bead
-   tensile network: 0.160 vs 0.168 ms per step at the 64 registers of an
-   unbounded build; 40 registers spill too much). */
-__global__ void __launch_bounds__(kChainMaxBlock, 5) k_step_chain(const StepArgs A, int terms) {
+/* At most 256 threads per block and 4 such blocks per SM, i.e. at most 64
+   registers: the kernel waits on dependent loads of contact partners, and
+   both resident warps and the registers that keep the next list index in
+   flight hide that latency (measured on the 1M-bead tensile network: 0.135 ms
+   per step at 64 registers, 0.144 ms at 48 registers, 0.154 ms at 76). */
+__global__ void __launch_bounds__(kChainMaxBlock, 4) k_step_chain(const StepArgs A, int terms) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
     const FnTile tile = A.tiles[blockIdx.x];
     const int b0 = tile.begin, n = tile.end - tile.begin;
@@ -732,9 +732,11 @@ __global__ void __launch_bounds__(kChainMaxBlock, 5) k_step_chain(const StepArgs
            through the windows */
         const int kd = __reduce_add_sync(0xffffffffu, nc) >> 5;
         const int nd = min(nc, kd);
+        int jn = nd > 0 ? A.list[i] : 0; /* next list index, loaded one item ahead */
         for (int k = 0; k < kd; ++k) {
             if (k < nd) {
-                const int j = A.list[(size_t)k * A.list_stride + i];
+                const int j = jn;
+                if (k + 1 < nd) jn = A.list[(size_t)(k + 1) * A.list_stride + i];
                 double Rx = 0.0, Ry = 0.0, Rz = 0.0;
                 if (contact_eval(N, A.pairs, p, A.pos_in[j], Rx, Ry, Rz)) {
                     Fx += Rx;
