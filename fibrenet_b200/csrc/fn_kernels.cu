@@ -727,11 +727,46 @@ __global__ void __launch_bounds__(kChainMaxBlock, 4) k_step_chain(const StepArgs
         if (active) s_pos_w[tid] = p;
         /* direct phase: every lane first evaluates the leading KD items of its
            own list, one list row per iteration (coalesced loads, no window
-           bookkeeping); KD is the warp's mean list length rounded down, so
-           most lanes are busy in it and only the longer lists' tails go
-           through the windows */
-        const int kd = __reduce_add_sync(0xffffffffu, nc) >> 5;
+           bookkeeping); the longer lists' tails then go through the windows.
+           KD is picked per warp among mean - 1 .. mean + 2 (mean rounded
+           down) to minimise 2 x KD + 3 x windows, a window costing about 1.5
+           direct iterations. */
+        int kd;
+        {
+            const int m = __reduce_add_sync(0xffffffffu, nc) >> 5;
+            kd = m;
+            int best = 2 * m + 3 * ((__reduce_add_sync(0xffffffffu, max(nc - m, 0)) + 31) >> 5);
+            for (int k = max(m - 1, 0); k <= m + 2; ++k) {
+                if (k == m) continue;
+                const int c = 2 * k + 3 * ((__reduce_add_sync(0xffffffffu, max(nc - k, 0)) + 31) >> 5);
+                if (c < best) {
+                    best = c;
+                    kd = k;
+                }
+            }
+        }
         const int nd = min(nc, kd);
+        const int nr = nc - nd; /* items left for the windows */
+        int off = nr;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= o) off += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, off, 31);
+        off -= nr; /* exclusive */
+        /* owner lane and list index of the first window's items, loaded
+           before the direct phase so their latency overlaps it */
+        int b_first = 0, j_first = 0;
+        if (total > 0) {
+            const int lim = min(32, total);
+            for (int w = off; w < min(off + nr, lim); ++w) s_map[w] = (unsigned char)lane;
+            __syncwarp();
+            b_first = lane < lim ? s_map[lane] : 0;
+            const int ob = __shfl_sync(0xffffffffu, off - nd, b_first);
+            if (lane < lim)
+                j_first = A.list[(size_t)(lane - ob) * A.list_stride + (b0 + (tid & ~31) + b_first)];
+        }
         int jn = nd > 0 ? A.list[i] : 0; /* next list index, loaded one item ahead */
         for (int k = 0; k < kd; ++k) {
             if (k < nd) {
@@ -745,26 +780,19 @@ __global__ void __launch_bounds__(kChainMaxBlock, 4) k_step_chain(const StepArgs
                 }
             }
         }
-        const int nr = nc - nd; /* items left for the windows */
-        int off = nr;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, off, o);
-            if (lane >= o) off += y;
-        }
-        const int total = __shfl_sync(0xffffffffu, off, 31);
-        off -= nr; /* exclusive */
-        __syncwarp();
         for (int base = 0; base < total; base += 32) {
             const int lim = min(base + 32, total);
-            for (int w = max(off, base); w < min(off + nr, lim); ++w) s_map[w - base] = (unsigned char)lane;
-            __syncwarp();
             const int w = base + lane;
-            const int b = w < lim ? s_map[lane] : 0;
-            const int ob = __shfl_sync(0xffffffffu, off - nd, b); /* list row = w - ob */
+            int b = b_first, j = j_first;
+            if (base > 0) {
+                for (int q = max(off, base); q < min(off + nr, lim); ++q) s_map[q - base] = (unsigned char)lane;
+                __syncwarp();
+                b = w < lim ? s_map[lane] : 0;
+                const int ob = __shfl_sync(0xffffffffu, off - nd, b); /* list row = w - ob */
+                if (w < lim) j = A.list[(size_t)(w - ob) * A.list_stride + (b0 + (tid & ~31) + b)];
+            }
             if (w < lim) {
                 const int ib = (tid & ~31) + b; /* block-local bead of the item */
-                const int j = A.list[(size_t)(w - ob) * A.list_stride + (b0 + ib)];
                 double Rx = 0.0, Ry = 0.0, Rz = 0.0;
                 const int acts = contact_eval(N, A.pairs, s_pos[ib], A.pos_in[j], Rx, Ry, Rz);
                 s_R[3 * lane] = Rx;
