@@ -133,18 +133,22 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.idx = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        self.path = None
 
     def start(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        import tempfile
         try:
-            self.f = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix=f"fn_clocks{self.idx}_", suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
                  "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                 stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            if self.path:
+                self.f.close()
+                os.remove(self.path)
 
     def stop(self):
         if self.proc is None:
@@ -160,6 +164,7 @@ class ClockSampler:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 9:
                 rows.append(parts)
+        os.remove(self.path)
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -181,7 +186,7 @@ def peaks():
 
 
 def algorithmic_bytes(m, half_pairs: float) -> float:
-    """Bytes one step must move (SURVEY 8(d) formula): per bead 4 state arrays
+    """Algorithmic bytes of one step: per bead 4 state arrays
     x 16 B read + written and 16 B of constants, per spring 16 B (+9 B HR_FL),
     per angle 20 B, list offsets 4 B per bead, 4 B per half-list pair."""
     import numpy as np
@@ -725,7 +730,7 @@ def run_plain(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
             "config": config_dict(m, args, {"graphs": True, "block_size": block,
                                             "l2": "working set in L2 (launch- and "
-                                            "latency-bound, not judged against HBM)"}),
+                                            "latency-bound, not measured against HBM)"}),
             "step_kernel_us": 1e3 * kt["step_ms"], "rebuild_us": 1e3 * kt["rebuild_ms"], "clocks": clk}
     print(json.dumps(line), flush=True)
 
