@@ -99,6 +99,24 @@ void parallel_for(long long n, F f) {
     for (auto& x : th) x.join();
 }
 
+/* Smallest i in [0, n) with bad(i), or -1: the checks run on host threads,
+   the answer is the one a sequential sweep gives. */
+template <class P>
+long long first_index(long long n, P bad) {
+    std::atomic<long long> best{n};
+    parallel_for(n, [&](long long b, long long e) {
+        for (long long i = b; i < e && i < best.load(std::memory_order_relaxed); ++i)
+            if (bad(i)) {
+                long long cur = best.load();
+                while (i < cur && !best.compare_exchange_weak(cur, i)) {
+                }
+                break;
+            }
+    });
+    const long long r = best.load();
+    return r < n ? r : -1;
+}
+
 template <class T>
 cudaError_t h2d(fn_ctx* c, DevBuf<T>& b, const HostArray<T>& v) {
     if (v.n == 0) return cudaSuccess;
@@ -285,18 +303,61 @@ int float_bits(float f) {
 void network_order(const fn_network_desc& d, const FnNet& N, bool reorder, std::vector<int>& order) {
     const int n = d.n_beads;
     order.resize(n);
-    std::iota(order.begin(), order.end(), 0);
-    if (!reorder || n == 0) return;
-    std::vector<int> root(n);
+    if (!reorder || n == 0) {
+        std::iota(order.begin(), order.end(), 0);
+        return;
+    }
+    auto morton_key = [&](int i) {
+        uint32_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            double x = d.pos[3 * i + a] / N.box[a] * 1024.0;
+            if (!(x >= 0.0)) x = 0.0;
+            if (x > 1023.0) x = 1023.0;
+            q[a] = (uint32_t)x;
+        }
+        const uint64_t m = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
+        return (m << 32) | (uint32_t)i;
+    };
     /* fibres listed bead after bead (every spring joins i and i + 1): each
-       component is a run of consecutive beads, labelled by one sweep */
-    bool runs = true;
-    for (int s = 0; s < d.n_springs && runs; ++s) runs = std::abs(d.s_p1[s] - d.s_p2[s]) == 1;
+       component is a run of consecutive beads starting where no spring
+       joins i - 1 and i; the runs are ordered by key and copied out on host
+       threads */
+    const bool runs =
+        first_index(d.n_springs, [&](long long s) { return std::abs(d.s_p1[s] - d.s_p2[s]) != 1; }) < 0;
     if (runs) {
         std::vector<unsigned char> link(n, 0); /* spring between i and i + 1 */
-        for (int s = 0; s < d.n_springs; ++s) link[std::min(d.s_p1[s], d.s_p2[s])] = 1;
-        for (int i = 0; i < n; ++i) root[i] = (i > 0 && link[i - 1]) ? root[i - 1] : i;
-    } else {
+        parallel_for(d.n_springs, [&](long long s0, long long s1) {
+            for (long long s = s0; s < s1; ++s)
+                __atomic_store_n(&link[std::min(d.s_p1[s], d.s_p2[s])], (unsigned char)1, __ATOMIC_RELAXED);
+        });
+        std::vector<int> starts;
+        for (int i = 0; i < n; ++i)
+            if (i == 0 || !link[i - 1]) starts.push_back(i);
+        const int R = (int)starts.size();
+        std::vector<uint64_t> keys(R);
+        parallel_for(R, [&](long long r0, long long r1) {
+            for (long long r = r0; r < r1; ++r) keys[r] = morton_key(starts[r]);
+        });
+        std::sort(keys.begin(), keys.end());
+        /* run r of the sorted list: first bead b, length up to the next start */
+        std::vector<int> first(R), len(R), out(R);
+        int acc = 0;
+        for (int r = 0; r < R; ++r) {
+            const int b = (int)(uint32_t)keys[r];
+            const int k = (int)(std::lower_bound(starts.begin(), starts.end(), b) - starts.begin());
+            first[r] = b;
+            len[r] = (k + 1 < R ? starts[k + 1] : n) - b;
+            out[r] = acc;
+            acc += len[r];
+        }
+        parallel_for(R, [&](long long r0, long long r1) {
+            for (long long r = r0; r < r1; ++r)
+                for (int t = 0; t < len[r]; ++t) order[out[r] + t] = first[r] + t;
+        });
+        return;
+    }
+    std::vector<int> root(n);
+    {
         std::vector<int> parent(n);
         std::iota(parent.begin(), parent.end(), 0);
         auto find = [&](int x) {
@@ -317,18 +378,8 @@ void network_order(const fn_network_desc& d, const FnNet& N, bool reorder, std::
        ascending order: a stable sort of the beads by (key of root, index)
        done as a counting sort in O(n + R log R) */
     std::vector<uint64_t> keys;
-    for (int i = 0; i < n; ++i) {
-        if (root[i] != i) continue;
-        uint32_t q[3];
-        for (int a = 0; a < 3; ++a) {
-            double x = d.pos[3 * i + a] / N.box[a] * 1024.0;
-            if (!(x >= 0.0)) x = 0.0;
-            if (x > 1023.0) x = 1023.0;
-            q[a] = (uint32_t)x;
-        }
-        uint64_t m = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
-        keys.push_back((m << 32) | (uint32_t)i);
-    }
+    for (int i = 0; i < n; ++i)
+        if (root[i] == i) keys.push_back(morton_key(i));
     std::sort(keys.begin(), keys.end());
     std::vector<int> start(n, 0); /* per root: first output slot */
     for (int i = 0; i < n; ++i) start[root[i]]++;
@@ -922,27 +973,40 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         if (r) return r;
         FnNet& N = c->nets_h[k];
         const int nt = d.settings.n_types;
-        for (int i = 0; i < d.n_beads; ++i) {
+        /* the first offending bead, spring or angle, as a sequential sweep
+           would report it */
+        const int nbk = d.n_beads, nsk = d.n_springs;
+        const long long bad_bead = first_index(nbk, [&](long long i) {
+            return d.type[i] < 0 || d.type[i] >= nt || !(d.mass[i] >= 0.0);
+        });
+        if (bad_bead >= 0) {
+            const long long i = bad_bead;
             if (d.type[i] < 0 || d.type[i] >= nt)
                 return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": bead " +
                                                std::to_string(i) + " has an undeclared type");
-            if (!(d.mass[i] >= 0.0))
-                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": negative mass");
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": negative mass");
         }
-        for (int s = 0; s < d.n_springs; ++s)
-            if (d.s_p1[s] < 0 || d.s_p1[s] >= d.n_beads || d.s_p2[s] < 0 || d.s_p2[s] >= d.n_beads)
-                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": spring " +
-                                               std::to_string(s) + " references a missing bead");
-        for (int a = 0; a < d.n_angles; ++a) {
-            int b[3] = {d.a_b1[a], d.a_b2[a], d.a_b3[a]};
-            for (int q = 0; q < 3; ++q)
-                if (b[q] < 0 || b[q] >= d.n_beads)
-                    return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": angle " +
-                                                   std::to_string(a) + " references a missing bead");
-            if (d.a_type[a] == 1 && (d.a_s1[a] < 0 || d.a_s1[a] >= d.n_springs || d.a_s2[a] < 0 ||
-                                     d.a_s2[a] >= d.n_springs))
-                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": HR_FL angle " +
-                                               std::to_string(a) + " references a missing spring");
+        const long long bad_spring = first_index(nsk, [&](long long s) {
+            return d.s_p1[s] < 0 || d.s_p1[s] >= nbk || d.s_p2[s] < 0 || d.s_p2[s] >= nbk;
+        });
+        if (bad_spring >= 0)
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": spring " +
+                                           std::to_string(bad_spring) + " references a missing bead");
+        auto angle_beads_bad = [&](long long a) {
+            return d.a_b1[a] < 0 || d.a_b1[a] >= nbk || d.a_b2[a] < 0 || d.a_b2[a] >= nbk ||
+                   d.a_b3[a] < 0 || d.a_b3[a] >= nbk;
+        };
+        const long long bad_angle = first_index(d.n_angles, [&](long long a) {
+            return angle_beads_bad(a) ||
+                   (d.a_type[a] == 1 &&
+                    (d.a_s1[a] < 0 || d.a_s1[a] >= nsk || d.a_s2[a] < 0 || d.a_s2[a] >= nsk));
+        });
+        if (bad_angle >= 0) {
+            if (angle_beads_bad(bad_angle))
+                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": angle " +
+                                               std::to_string(bad_angle) + " references a missing bead");
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": HR_FL angle " +
+                                           std::to_string(bad_angle) + " references a missing spring");
         }
         const int npairs = nt * (nt + 1) / 2;
         N.pair_base = (int)c->pairs_h.size();
@@ -960,13 +1024,21 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         /* largest listing radius (squared): cutoff for lj/st, the largest
            radius + the largest skin for hs (kernel.cl:632-650) */
         double rmax = 0.0, smax = 0.0, gap = 1e300;
-        for (int i = 0; i < d.n_beads; ++i) {
-            const float rad = (float)d.radius[i];
-            const float skin = (float)((double)rad + d.settings.skin_ratio);
-            rmax = std::max(rmax, (double)rad);
-            smax = std::max(smax, (double)skin);
-            gap = std::min(gap, (double)skin - (double)rad);
-        }
+        std::mutex red;
+        parallel_for(d.n_beads, [&](long long i0, long long i1) {
+            double r = 0.0, sm = 0.0, g = 1e300;
+            for (long long i = i0; i < i1; ++i) {
+                const float rad = (float)d.radius[i];
+                const float skin = (float)((double)rad + d.settings.skin_ratio);
+                r = std::max(r, (double)rad);
+                sm = std::max(sm, (double)skin);
+                g = std::min(g, (double)skin - (double)rad);
+            }
+            std::lock_guard<std::mutex> lk(red);
+            rmax = std::max(rmax, r);
+            smax = std::max(smax, sm);
+            gap = std::min(gap, g);
+        });
         c->info[k].skin_gap = gap;
         c->info[k].any_cut = any_cut;
         c->info[k].any_hs = any_hs;
@@ -1060,10 +1132,12 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         std::vector<int> order;
         network_order(nets[k], c->nets_h[k], c->cfg.reorder != 0, order);
         const int base = c->info[k].bead_begin;
-        for (int q = 0; q < (int)order.size(); ++q) {
-            c->perm[base + q] = base + order[q];
-            c->inv[base + order[q]] = base + q;
-        }
+        parallel_for((long long)order.size(), [&](long long q0, long long q1) {
+            for (long long q = q0; q < q1; ++q) {
+                c->perm[base + q] = base + order[q];
+                c->inv[base + order[q]] = base + (int)q;
+            }
+        });
     }
 
     /* bead arrays in internal order */
@@ -1096,14 +1170,52 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         });
     }
 
-    /* springs and angles keep their (concatenated) file order */
-    std::vector<int2> sp_ends(ns);
+    /* the device arrays exist from here on: the bead arrays go to the device
+       on a helper thread while this one converts the bonds */
+    allocator.join();
+    if (alloc_err != cudaSuccess)
+        return fail(c, alloc_err == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA,
+                    alloc_what + ": " + cudaGetErrorString(alloc_err));
+    c->cur = 0;
+    cudaError_t copy_err[2] = {cudaSuccess, cudaSuccess};
+    std::string copy_what[2];
+#define CP(k, call)                           \
+    do {                                      \
+        if ((copy_err[k] = (call)) != cudaSuccess) { \
+            copy_what[k] = #call;             \
+            return;                           \
+        }                                     \
+    } while (0)
+    std::thread bead_copier([&] {
+        if ((copy_err[0] = cudaSetDevice(c->cfg.device)) != cudaSuccess) return;
+        CP(0, h2d(c, c->pos[0], pos));
+        CP(0, h2d(c, c->img[0], img));
+        CP(0, cudaMemcpyAsync(c->pos[1].p, c->pos[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
+        CP(0, cudaMemcpyAsync(c->img[1].p, c->img[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
+        CP(0, h2d(c, c->vold, vold));
+        CP(0, h2d(c, c->force, force));
+        CP(0, h2d(c, c->vel, vel));
+        CP(0, h2d(c, c->binfo, binfo));
+        CP(0, h2d(c, c->nets, c->nets_h));
+        CP(0, h2d(c, c->pairs, c->pairs_h));
+        CP(0, cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * FN_CNT_N, c->stream));
+        CP(0, cudaMemsetAsync(c->list_count.p, 0, sizeof(int) * (size_t)nb, c->stream));
+        CP(0, cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
+        CP(0, cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
+    });
+
+    /* springs and angles keep their (concatenated) file order; the host
+       copies the engine keeps are filled in place */
     std::vector<signed char> sp_type(ns), sp_status(ns, 1);
-    c->sp_par_h.assign(ns, make_float4(0, 0, 0, 0));
-    std::vector<int4> an_b(na);
-    std::vector<int2> an_s(na);
+    c->sp_ends_h.resize(ns);
+    c->sp_par_h.resize(ns);
+    c->an_b_h.resize(na);
+    c->an_s_h.resize(na);
+    c->an_par_h.resize(na);
     std::vector<signed char> an_status(na, 1);
-    c->an_par_h.assign(na, make_float2(0, 0));
+    std::vector<int2>& sp_ends = c->sp_ends_h;
+    std::vector<int4>& an_b = c->an_b_h;
+    std::vector<int2>& an_s = c->an_s_h;
     for (int k = 0; k < n_networks; ++k) {
         const fn_network_desc& d = nets[k];
         const NetHost& h = c->info[k];
@@ -1127,56 +1239,28 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         }
         });
     }
-
-    c->sp_ends_h = sp_ends;
     c->incidence_ready = false;
-    c->an_b_h = an_b;
-    c->an_s_h = an_s;
-    allocator.join();
-    if (alloc_err != cudaSuccess)
-        return fail(c, alloc_err == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA,
-                    alloc_what + ": " + cudaGetErrorString(alloc_err));
-    c->cur = 0;
-    /* host-to-device copies on a helper thread while this one builds the
-       chain records */
-    cudaError_t copy_err = cudaSuccess;
-    std::string copy_what;
-    std::thread copier([&] {
-        if ((copy_err = cudaSetDevice(c->cfg.device)) != cudaSuccess) return;
-#define CP(call)                          \
-    do {                                  \
-        if ((copy_err = (call)) != cudaSuccess) { \
-            copy_what = #call;            \
-            return;                       \
-        }                                 \
-    } while (0)
-        CP(h2d(c, c->pos[0], pos));
-        CP(h2d(c, c->img[0], img));
-        CP(cudaMemcpyAsync(c->pos[1].p, c->pos[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
-        CP(cudaMemcpyAsync(c->img[1].p, c->img[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
-        CP(h2d(c, c->vold, vold));
-        CP(h2d(c, c->force, force));
-        CP(h2d(c, c->vel, vel));
-        CP(h2d(c, c->binfo, binfo));
-        CP(h2d(c, c->sp_ends, sp_ends));
-        CP(h2d(c, c->sp_par, c->sp_par_h));
-        CP(h2d(c, c->sp_type, sp_type));
-        CP(h2d(c, c->sp_status, sp_status));
-        CP(h2d(c, c->an_b, an_b));
-        CP(h2d(c, c->an_s, an_s));
-        CP(h2d(c, c->an_par, c->an_par_h));
-        CP(h2d(c, c->an_status, an_status));
-        CP(h2d(c, c->nets, c->nets_h));
-        CP(h2d(c, c->pairs, c->pairs_h));
-        CP(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * FN_CNT_N, c->stream));
-        CP(cudaMemsetAsync(c->list_count.p, 0, sizeof(int) * (size_t)nb, c->stream));
-        CP(cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
-        CP(cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
-#undef CP
+
+    /* the bond arrays go to the device on a second helper thread while this
+       one builds the chain records */
+    std::thread bond_copier([&] {
+        if ((copy_err[1] = cudaSetDevice(c->cfg.device)) != cudaSuccess) return;
+        CP(1, h2d(c, c->sp_ends, sp_ends));
+        CP(1, h2d(c, c->sp_par, c->sp_par_h));
+        CP(1, h2d(c, c->sp_type, sp_type));
+        CP(1, h2d(c, c->sp_status, sp_status));
+        CP(1, h2d(c, c->an_b, an_b));
+        CP(1, h2d(c, c->an_s, an_s));
+        CP(1, h2d(c, c->an_par, c->an_par_h));
+        CP(1, h2d(c, c->an_status, an_status));
     });
+#undef CP
     c->chain = c->cfg.chain_mode != 2 && build_chain(c, sp_ends, sp_type, an_b, an_s);
-    copier.join();
-    if (copy_err != cudaSuccess) return fail(c, FN_ERR_CUDA, copy_what + ": " + cudaGetErrorString(copy_err));
+    bead_copier.join();
+    bond_copier.join();
+    for (int k = 0; k < 2; ++k)
+        if (copy_err[k] != cudaSuccess)
+            return fail(c, FN_ERR_CUDA, copy_what[k] + ": " + cudaGetErrorString(copy_err[k]));
     int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128);
     if (r) return r;
     r = verlet_setup(c);
