@@ -264,7 +264,7 @@ class Simulation:
 
     # --- state
     def get(self, field: str) -> np.ndarray:
-        out = np.zeros((self.nb, 3), np.float64)
+        out = np.empty((self.nb, 3), np.float64)  # every element is written by fn_download
         self._check(self.lib.fn_download(self.h, FIELDS[field], out.ctypes.data_as(_D)))
         return out
 
