@@ -1074,6 +1074,10 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     c->na = na;
     c->ncells = ncells;
     c->list_stride = (int)((nb + 31) / 32 * 32);
+    /* the export's copy of the numbering is rebuilt on first use; freed
+       here, before the helper thread below starts to allocate (both update
+       the context's device-byte count) */
+    dfree(c, c->inv_d);
     /* device allocations on a helper thread while this one orders and
        converts the model (the sizes are known from here on) */
     cudaError_t alloc_err = cudaSuccess;
@@ -1127,7 +1131,6 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     /* bead order */
     c->perm.assign(nb, 0);
     c->inv.assign(nb, 0);
-    dfree(c, c->inv_d); /* the export's copy of the numbering, rebuilt on first use */
     for (int k = 0; k < n_networks; ++k) {
         std::vector<int> order;
         network_order(nets[k], c->nets_h[k], c->cfg.reorder != 0, order);
