@@ -297,9 +297,10 @@ FN_API int fn_step_series(fn_ctx* ctx, int nsteps, int every, int net, int react
                           int with_energy, double* host_rows);
 
 /* The observables of fn_observe for callers that cannot allocate device
-   memory when they need them, e.g. code that runs while a CUDA graph is being
-   captured or inside a loop where a cudaMalloc (which may synchronise the
-   device) is not allowed.  No counterpart in the reference.  Writes
+   memory when they need them: a host loop or callback that must not
+   synchronise the device (cudaMalloc and cudaFree may), or an application
+   whose device memory all belongs to its own allocator.  No counterpart in
+   the reference.  Writes
    {reaction x, y, z, broken springs, dead angles} as 5 doubles to the
    caller's device buffer out_device, asynchronously on the context's stream
    (read it after fn_sync).  Calls no cudaMalloc/cudaFree: its scratch is a

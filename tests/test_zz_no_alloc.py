@@ -1,7 +1,7 @@
 """fn_observe_noalloc: the observables reduction for callers that cannot
-allocate device memory at the point of the call (for instance while a CUDA
-graph is being captured, or in a loop where a cudaMalloc and the device
-synchronisation it may cause are not allowed).  It must give fn_observe's
+allocate device memory at the point of the call (a loop or callback that must
+not synchronise the device, as cudaMalloc and cudaFree may, or an application
+whose device memory all belongs to its own allocator).  It must give fn_observe's
 results, call after call, with its scratch in the library's static array and
 without any device allocation.  Collected last so that a failure here leaves
 every other test already run."""
