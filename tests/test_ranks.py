@@ -58,3 +58,43 @@ def test_two_gloo_ranks_aggregate():
         assert p.exitcode == 0
     # (1000 + 2000) bead-steps over the slowest 200 ms
     assert out[0] == out[1] == (15000.0, 7.0)
+
+
+def _worker_leaves(rank, world, port, out):
+    import datetime
+    import time
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        # leaves between steps, with no collective of its own in flight
+        os._exit(0)
+    t0 = time.monotonic()
+    try:
+        job_rate(1000.0, 100.0, dist)
+        out[rank] = ("no error", time.monotonic() - t0)
+    except Exception as e:  # noqa: BLE001 - any error ends the wait
+        out[rank] = (type(e).__name__, time.monotonic() - t0)
+    os._exit(0)
+
+
+def test_rank_that_leaves_ends_the_others_collective_with_an_error():
+    """A rank that exits between steps: the remaining rank's next timing
+    collective returns an error within the process group's short timeout
+    instead of waiting for good."""
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_leaves, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    what, waited = out[0]
+    assert what != "no error"
+    assert waited < 60.0
