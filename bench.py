@@ -195,9 +195,14 @@ def algorithmic_bytes(m, half_pairs: float) -> float:
             + (m.n_beads + 1) * 4 + half_pairs * 4)
 
 
-def layout_bytes(m, half_pairs: float) -> float:
-    """Bytes the step kernel's own layout moves at minimum (FP64 positions)."""
+def layout_bytes(m, half_pairs: float, chain: bool = True) -> float:
+    """Bytes the step kernel's own layout moves at minimum (FP64 positions).
+    Chain form: position and image (double4) and force and velocity_old
+    (float4) read and written, 26 B of bond records, the list length and the
+    list entries per bead.  Otherwise the incidence layout."""
     n, ns, na = m.n_beads, m.n_springs, m.n_angles
+    if chain:
+        return n * (2 * 32 + 2 * 16) * 2 + n * 26 + n * 4 + 2 * half_pairs * 4
     state = n * (2 * 32 + 2 * 32 + 2 * 16 + 2 * 16)  # pos, img double4 r/w; v_old, F float4 r/w
     bonds = ns * (8 + 16 + 2) + na * (16 + 8 + 8 + 1)
     incid = (n + 1) * 8 + 2 * ns * 4 + 3 * na * 4
@@ -439,7 +444,7 @@ def run_ours(args):
                          "peak_kind": peak_kind,
                          "kernel": "k_step (force + kick + drift, one launch per step)",
                          "algorithmic_bytes_per_launch": alg,
-                         "layout_bytes_per_launch": layout_bytes(m, half_pairs),
+                         "layout_bytes_per_launch": layout_bytes(m, half_pairs, stats["bond_path"] == 2),
                          "step_kernel_ms": step_ms, "rebuild_ms": kt["rebuild_ms"],
                          "traffic": (traffic_per_bead * nb) if traffic_per_bead else None},
             "cpu_baseline": cpu,
