@@ -22,6 +22,7 @@
 #include <numeric>
 #include <thread>
 #include <string>
+#include <system_error>
 #include <vector>
 
 #include "../../include/fibrenet.h"
@@ -91,13 +92,28 @@ void parallel_for(long long n, F f) {
         return;
     }
     std::vector<std::thread> th;
+    th.reserve((size_t)nt);
     const long long chunk = (n + nt - 1) / nt;
     for (long long t = 0; t < nt; ++t) {
         const long long b = t * chunk, e = std::min(n, b + chunk);
-        if (b < e) th.emplace_back([=] { f(b, e); });
+        if (b >= e) continue;
+        try {
+            th.emplace_back([=] { f(b, e); });
+        } catch (const std::system_error&) {
+            f(b, e); /* no thread to be had: this chunk on the calling thread */
+        }
     }
     for (auto& x : th) x.join();
 }
+
+/* Joins a helper thread when the scope ends, on every path out of it: a
+   joinable std::thread that is destroyed ends the process. */
+struct JoinOnExit {
+    std::thread& t;
+    ~JoinOnExit() {
+        if (t.joinable()) t.join();
+    }
+};
 
 /* Smallest i in [0, n) with bad(i), or -1: the checks run on host threads,
    the answer is the one a sequential sweep gives. */
@@ -944,7 +960,8 @@ FN_API void fn_destroy(fn_ctx* c) {
 
 FN_API const char* fn_last_error(const fn_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
+/* fn_upload's work; fn_upload turns the host's exceptions into status codes. */
+static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     if (c) c->state_version++;
     if (!c || n_networks <= 0 || !nets) return fail(c, FN_ERR_ARG, "fn_upload: bad arguments");
     CK(cudaSetDevice(c->cfg.device));
@@ -1125,6 +1142,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         AL(dalloc(c, c->en_out, fn::FN_EN_N));
 #undef AL
     });
+    JoinOnExit join_allocator{allocator};
 
     c->grid_update_freq = c->info[0].grid_update_freq;
 
@@ -1206,6 +1224,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         CP(0, cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
         CP(0, cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
     });
+    JoinOnExit join_bead_copier{bead_copier};
 
     /* springs and angles keep their (concatenated) file order; the host
        copies the engine keeps are filled in place */
@@ -1257,6 +1276,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
         CP(1, h2d(c, c->an_par, c->an_par_h));
         CP(1, h2d(c, c->an_status, an_status));
     });
+    JoinOnExit join_bond_copier{bond_copier};
 #undef CP
     c->chain = c->cfg.chain_mode != 2 && build_chain(c, sp_ends, sp_type, an_b, an_s);
     bead_copier.join();
@@ -1273,6 +1293,18 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     c->rebuilds_done = 0;
     c->uploaded = true;
     return FN_OK;
+}
+
+FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
+    try {
+        return upload_model(c, n_networks, nets);
+    } catch (const std::bad_alloc&) {
+        return fail(c, FN_ERR_OOM, "fn_upload: out of host memory");
+    } catch (const std::system_error& e) {
+        return fail(c, FN_ERR_OOM, std::string("fn_upload: no host thread: ") + e.what());
+    } catch (const std::exception& e) {
+        return fail(c, FN_ERR_ARG, std::string("fn_upload: ") + e.what());
+    }
 }
 
 FN_API int fn_step(fn_ctx* c, int nsteps) {
