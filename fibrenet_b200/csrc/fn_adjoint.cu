@@ -823,6 +823,7 @@ extern "C" {
 
 FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint_every, int reaction_type,
                               double* reaction) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (nsamples <= 0 || every <= 0 || checkpoint_every <= 0 || checkpoint_every % every != 0)
@@ -880,11 +881,13 @@ FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint
     CK(cudaStreamSynchronize(c->stream));
     S->version = c->state_version;
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double* grad_spring_k,
                                double* grad_spring_rest, double* grad_angle_k, double* grad_pos0,
                                double* grad_vel0) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     AdjointState* S = c->adj;
@@ -1007,14 +1010,17 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
         }
     }
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_adjoint_release(fn_ctx* c) {
+    FN_TRY
     if (!c) return FN_ERR_ARG;
     cudaSetDevice(c->cfg.device);
     cudaStreamSynchronize(c->stream);
     adjoint_free(c);
     return FN_OK;
+    FN_CATCH(c)
 }
 
 }  // extern "C"

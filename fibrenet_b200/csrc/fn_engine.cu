@@ -44,11 +44,6 @@ double list_r2(const NetHost& h, double cutoff_sq, double smax) {
     return r2;
 }
 
-int getadress_h(int t1, int t2, int size) {
-    return (t1 < t2) ? ((size * t1) + t2 - ((t1 * (t1 + 1)) / 2))
-                     : ((size * t2) + t1 - ((t2 * (t2 + 1)) / 2));
-}
-
 uint32_t spread10(uint32_t v) {
     v &= 0x3ff;
     v = (v | (v << 16)) & 0x030000FF;
@@ -919,6 +914,7 @@ using namespace fnh;
 extern "C" {
 
 FN_API int fn_create(const fn_config* cfg, fn_ctx** out) {
+    FN_TRY
     if (!cfg || !out) return FN_ERR_ARG;
     *out = nullptr;
     fn_ctx* c = new fn_ctx();
@@ -946,6 +942,7 @@ FN_API int fn_create(const fn_config* cfg, fn_ctx** out) {
     }
     *out = c;
     return FN_OK;
+    FN_CATCH(nullptr)
 }
 
 FN_API void fn_destroy(fn_ctx* c) {
@@ -1308,6 +1305,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
 }
 
 FN_API int fn_step(fn_ctx* c, int nsteps) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1329,9 +1327,11 @@ FN_API int fn_step(fn_ctx* c, int nsteps) {
     }
     c->steps_done += nsteps;
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_rebuild_contacts(fn_ctx* c) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1341,18 +1341,22 @@ FN_API int fn_rebuild_contacts(fn_ctx* c) {
         CK(cudaStreamSynchronize(c->stream));
     }
     return do_rebuild(c);
+    FN_CATCH(c)
 }
 
 FN_API int fn_reset_energy(fn_ctx* c) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
     CK(fn::launch_reset_energy(c->force.p, c->vel.p, c->vold.p, (int)c->nb, c->stream));
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_sync(fn_ctx* c) {
+    FN_TRY
     if (!c) return FN_ERR_ARG;
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
@@ -1361,9 +1365,11 @@ FN_API int fn_sync(fn_ctx* c) {
     CK(cudaMemcpy(&bad, c->counters.p + FN_CNT_NONFINITE, sizeof bad, cudaMemcpyDeviceToHost));
     if (bad) return fail(c, FN_ERR_NONFINITE, "non-finite force detected in " + std::to_string(bad) + " bead-steps");
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_device_view(fn_ctx* c, int field, fn_view* out) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (!out) return fail(c, FN_ERR_ARG, "fn_device_view: null output");
@@ -1380,9 +1386,11 @@ FN_API int fn_device_view(fn_ctx* c, int field, fn_view* out) {
     default: return fail(c, FN_ERR_ARG, "fn_device_view: unknown field");
     }
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_download(fn_ctx* c, int field, double* host) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (!host) return fail(c, FN_ERR_ARG, "fn_download: null host pointer");
@@ -1409,9 +1417,11 @@ FN_API int fn_download(fn_ctx* c, int field, double* host) {
     CK(cudaMemcpyAsync(host, c->export_xyz.p, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_set_beads(fn_ctx* c, int field, const double* host) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1448,9 +1458,11 @@ FN_API int fn_set_beads(fn_ctx* c, int field, const double* host) {
     }
     CK(cudaMemcpy(b->p, tmp.data(), sizeof(float4) * nb, cudaMemcpyHostToDevice));
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_set_mass(fn_ctx* c, const double* mass) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1469,9 +1481,11 @@ FN_API int fn_set_mass(fn_ctx* c, const double* mass) {
     }
     CK(cudaMemcpy(c->img[c->cur].p, tmp.data(), sizeof(double4) * nb, cudaMemcpyHostToDevice));
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1497,10 +1511,12 @@ FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
     r = verlet_setup(c);
     if (r) return r;
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_set_springs(fn_ctx* c, const double* rest, const double* k, const double* c1,
                           const double* c2) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1521,9 +1537,11 @@ FN_API int fn_set_springs(fn_ctx* c, const double* rest, const double* k, const 
         CK(cudaMemcpy(c->ch_sp.p, chs.data(), sizeof(float4) * c->nb, cudaMemcpyHostToDevice));
     }
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_set_angles(fn_ctx* c, const double* theta0, const double* k) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1541,9 +1559,11 @@ FN_API int fn_set_angles(fn_ctx* c, const double* theta0, const double* k) {
         CK(cudaMemcpy(c->ch_an.p, cha.data(), sizeof(float2) * c->nb, cudaMemcpyHostToDevice));
     }
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_download_status(fn_ctx* c, int* spring_status, int* angle_status) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1568,9 +1588,11 @@ FN_API int fn_download_status(fn_ctx* c, int* spring_status, int* angle_status) 
     if (angle_status)
         for (long long q = 0; q < c->na; ++q) angle_status[q] = a[q];
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_status) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1599,6 +1621,7 @@ FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_s
         CK(cudaMemcpy(c->an_status.p, a.data(), c->na, cudaMemcpyHostToDevice));
     }
     return FN_OK;
+    FN_CATCH(c)
 }
 
 namespace {
@@ -1667,6 +1690,7 @@ int energy_async(fn_ctx* c, int net, double* out) {
 }  // namespace
 
 FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_observe: bad arguments");
@@ -1680,10 +1704,12 @@ FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out
     out->broken = (long long)res[3];
     out->angles_dead = (long long)res[4];
     return FN_OK;
+    FN_CATCH(c)
 }
 
 
 FN_API int fn_energy_eval(fn_ctx* c, int net, fn_energy* out) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_energy_eval: bad arguments");
@@ -1702,10 +1728,12 @@ FN_API int fn_energy_eval(fn_ctx* c, int net, fn_energy* out) {
     for (int k = 0; k < 9; ++k) out->virial[k] = res[fn::FN_EN_VIRIAL + k];
     out->contacts = (long long)res[fn::FN_EN_CONTACTS];
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_step_series(fn_ctx* c, int nsteps, int every, int net, int reaction_type,
                           int with_energy, double* host_rows) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (nsteps <= 0 || every <= 0 || net < 0 || net >= c->n_nets || !host_rows)
@@ -1738,9 +1766,11 @@ FN_API int fn_step_series(fn_ctx* c, int nsteps, int every, int net, int reactio
     CK(cudaStreamSynchronize(c->stream));
     for (long long q = 0; q < rows; ++q) host_rows[(size_t)q * width] = steps_done[q];
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
+    FN_TRY
     if (!c || !out) return FN_ERR_ARG;
     std::memset(out, 0, sizeof *out);
     out->block_size = c->block;
@@ -1762,11 +1792,13 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     out->list_overflow = (long long)cnt[FN_CNT_LIST_OVERFLOW];
     if (cnt[FN_CNT_NONFINITE]) c->err = "non-finite force detected";
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API long long fn_n_cells(fn_ctx* c) { return c ? c->ncells : -1; }
 
 FN_API int fn_get_cells(fn_ctx* c, int* bead_cell, int* cell_count, long long n_cells) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1782,9 +1814,11 @@ FN_API int fn_get_cells(fn_ctx* c, int* bead_cell, int* cell_count, long long n_
         CK(cudaStreamSynchronize(c->stream));
     }
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_get_lists(fn_ctx* c, int* count, int* partners, int cap) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     CK(cudaSetDevice(c->cfg.device));
@@ -1807,20 +1841,24 @@ FN_API int fn_get_lists(fn_ctx* c, int* count, int* partners, int cap) {
         }
     }
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_get_permutation(fn_ctx* c, int* perm) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (!perm) return FN_ERR_ARG;
     std::memcpy(perm, c->perm.data(), sizeof(int) * c->nb);
     return FN_OK;
+    FN_CATCH(c)
 }
 
 /* Starts (on != 0) or stops a timing window: while on, every step-kernel
    launch and every rebuild is bracketed by CUDA events on the context's
    stream; fn_kernel_time averages the window. */
 FN_API int fn_enable_timing(fn_ctx* c, int on) {
+    FN_TRY
     if (!c) return FN_ERR_ARG;
     if (on) {
         CK(cudaSetDevice(c->cfg.device));
@@ -1831,10 +1869,12 @@ FN_API int fn_enable_timing(fn_ctx* c, int on) {
     }
     c->timing = on != 0;
     return FN_OK;
+    FN_CATCH(c)
 }
 
 FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, double* rebuild_ms,
                           long long* rebuilds) {
+    FN_TRY
     if (!c) return FN_ERR_ARG;
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
@@ -1854,6 +1894,7 @@ FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, doubl
     if (rebuild_ms) *rebuild_ms = c->ev_rebuild.empty() ? 0.0 : tr / (double)c->ev_rebuild.size();
     if (rebuilds) *rebuilds = (long long)c->ev_rebuild.size();
     return FN_OK;
+    FN_CATCH(c)
 }
 
 /* Block-size tuner: for each candidate the same `steps_per_trial` steps run
@@ -1861,6 +1902,7 @@ FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, doubl
    simulation does not advance), timed with CUDA events; the fastest block
    size is kept. */
 FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (steps_per_trial <= 0) return fail(c, FN_ERR_ARG, "fn_autotune: steps_per_trial must be positive");
@@ -1932,11 +1974,13 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     c->timing = timing0;
     if (r) return r;
     return set_block(c, best);
+    FN_CATCH(c)
 }
 
 /* Forces alone at the current positions (zeroed, no base term), for the
    one-step parity checks: terms bit 0 springs, 1 angles, 2 contacts. */
 FN_API int fn_forces_only(fn_ctx* c, int terms) {
+    FN_TRY
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1947,6 +1991,7 @@ FN_API int fn_forces_only(fn_ctx* c, int terms) {
     else
         CK(fn::launch_forces_only(A, c->ntiles, c->block, terms, c->stream));
     return FN_OK;
+    FN_CATCH(c)
 }
 
 }  // extern "C"
@@ -1991,6 +2036,7 @@ int noalloc_scratch(fn_ctx* c, double** out) {
 }  // namespace
 
 extern "C" FN_API int fn_observe_noalloc(fn_ctx* c, int net, int reaction_type, double* out_device) {
+    FN_TRY
     int r = check_ready(c);
     if (r) return r;
     if (!out_device || net < 0 || net >= c->n_nets)
@@ -2027,4 +2073,5 @@ extern "C" FN_API int fn_observe_noalloc(fn_ctx* c, int net, int reaction_type, 
     O.partial = scratch;
     CK(fn::launch_observe(O, (int)nblocks, out_device, c->stream));
     return FN_OK;
+    FN_CATCH(c)
 }

@@ -9,6 +9,9 @@
 
 #include <map>
 #include <string>
+#include <system_error>
+#include <new>
+#include <stdexcept>
 #include <tuple>
 #include <utility>
 #include <vector>
@@ -138,6 +141,23 @@ struct fn_ctx {
 namespace fnh {
 
 int fail(fn_ctx* c, int code, const std::string& msg);
+
+/* Entry points of the C ABI wrap their bodies in FN_TRY ... FN_CATCH(ctx) so
+   that no C++ exception (host memory or threads running out) crosses the
+   boundary: it becomes FN_ERR_OOM or FN_ERR_ARG with the reason in
+   fn_last_error. */
+#define FN_TRY try {
+#define FN_CATCH(ctx)                                                                     \
+    }                                                                                     \
+    catch (const std::bad_alloc&) {                                                       \
+        return fnh::fail(ctx, FN_ERR_OOM, "out of host memory");                          \
+    }                                                                                     \
+    catch (const std::system_error& e_) {                                                 \
+        return fnh::fail(ctx, FN_ERR_OOM, std::string("host resources: ") + e_.what());   \
+    }                                                                                     \
+    catch (const std::exception& e_) {                                                    \
+        return fnh::fail(ctx, FN_ERR_ARG, e_.what());                                     \
+    }
 
 #define CK(call)                                                                          \
     do {                                                                                  \
