@@ -67,10 +67,27 @@ void direction(Rng& rng, double tilt_deg, int orient, double d[3]) {
 
 }  // namespace
 
+static int place_fibres(unsigned long long seed, int n_fibres, int beads, const double box[3],
+                        int periodic_mask, double zlo, double zhi, double tilt_deg, int orient,
+                        double spacing, double min_sep, int max_tries, double* out);
+
+/* fn_place_fibres behind a guard: host memory running out returns 3 instead
+   of an exception crossing the C ABI. */
 extern "C" FN_GEN_API int fn_place_fibres(unsigned long long seed, int n_fibres, int beads,
                                           const double box[3], int periodic_mask, double zlo,
                                           double zhi, double tilt_deg, int orient, double spacing,
                                           double min_sep, int max_tries, double* out) {
+    try {
+        return place_fibres(seed, n_fibres, beads, box, periodic_mask, zlo, zhi, tilt_deg, orient,
+                            spacing, min_sep, max_tries, out);
+    } catch (const std::exception&) {
+        return 3;
+    }
+}
+
+static int place_fibres(unsigned long long seed, int n_fibres, int beads, const double box[3],
+                        int periodic_mask, double zlo, double zhi, double tilt_deg, int orient,
+                        double spacing, double min_sep, int max_tries, double* out) {
     if (n_fibres < 0 || beads <= 0 || !box || !out || max_tries <= 0) return 1;
     Rng rng(seed);
     const bool per[3] = {(periodic_mask & 1) != 0, (periodic_mask & 2) != 0, (periodic_mask & 4) != 0};

@@ -688,6 +688,14 @@ FN_IO_API int fn_input_read(const char* input_path, int strict, fn_input** out, 
         copy_err(e.msg, err, err_len);
         delete in;
         return FN_ERR_ARG;
+    } catch (const std::bad_alloc&) {
+        copy_err("out of host memory", err, err_len);
+        delete in;
+        return FN_ERR_OOM;
+    } catch (const std::exception& e) {
+        copy_err(e.what(), err, err_len);
+        delete in;
+        return FN_ERR_ARG;
     }
     copy_err("", err, err_len);
     *out = in;
@@ -748,7 +756,22 @@ FN_IO_API const char* fn_input_type_name(const fn_input* in, int t) {
 
 FN_IO_API const char* fn_input_output_stem(const fn_input* in) { return in ? in->stem.c_str() : nullptr; }
 
+static int run_input(const char* input_path, int device, int strict, char* err, int err_len);
+
+/* The Run flow behind a guard: no C++ exception crosses the C ABI. */
 FN_IO_API int fn_run_input(const char* input_path, int device, int strict, char* err, int err_len) {
+    try {
+        return run_input(input_path, device, strict, err, err_len);
+    } catch (const std::bad_alloc&) {
+        copy_err("out of host memory", err, err_len);
+        return FN_ERR_OOM;
+    } catch (const std::exception& e) {
+        copy_err(e.what(), err, err_len);
+        return FN_ERR_ARG;
+    }
+}
+
+static int run_input(const char* input_path, int device, int strict, char* err, int err_len) {
     fn_input* in = nullptr;
     int rc = fn_input_read(input_path, strict, &in, err, err_len);
     if (rc) return rc;

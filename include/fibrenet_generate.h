@@ -19,7 +19,8 @@ extern "C" {
    axis a periodic.  orient 0: direction uniform in xy with a z tilt uniform in
    +-tilt_deg; 1: uniform on the sphere.  min_sep > 0 keeps every bead at least
    that far from the beads placed before it.  Returns 0, 1 on bad arguments,
-   2 when a fibre found no place in max_tries draws. */
+   2 when a fibre found no place in max_tries draws, 3 when host memory runs
+   out. */
 FN_GEN_API int fn_place_fibres(unsigned long long seed, int n_fibres, int beads, const double box[3],
                                int periodic_mask, double zlo, double zhi, double tilt_deg,
                                int orient, double spacing, double min_sep, int max_tries,
