@@ -824,6 +824,7 @@ extern "C" {
 FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint_every, int reaction_type,
                               double* reaction) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_adjoint_forward");
     int r = check_ready(c);
     if (r) return r;
     if (nsamples <= 0 || every <= 0 || checkpoint_every <= 0 || checkpoint_every % every != 0)
@@ -888,6 +889,7 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
                                double* grad_spring_rest, double* grad_angle_k, double* grad_pos0,
                                double* grad_vel0) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_adjoint_backward");
     int r = check_ready(c);
     if (r) return r;
     AdjointState* S = c->adj;

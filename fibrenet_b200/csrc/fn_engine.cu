@@ -775,6 +775,7 @@ cudaEvent_t next_event(fn_ctx* c) {
 }
 
 int do_rebuild(fn_ctx* c) {
+    fnh::NvtxRange nvtx_range_("fn_rebuild");
     fn::RebuildArgs R = rebuild_args(c);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->timing) {
@@ -959,6 +960,7 @@ FN_API const char* fn_last_error(const fn_ctx* c) { return c ? c->err.c_str() : 
 
 /* fn_upload's work; fn_upload turns the host's exceptions into status codes. */
 static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
+    fnh::NvtxRange nvtx_range_("fn_upload");
     if (c) c->state_version++;
     if (!c || n_networks <= 0 || !nets) return fail(c, FN_ERR_ARG, "fn_upload: bad arguments");
     CK(cudaSetDevice(c->cfg.device));
@@ -1306,6 +1308,7 @@ FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
 
 FN_API int fn_step(fn_ctx* c, int nsteps) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_step");
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
@@ -1391,6 +1394,7 @@ FN_API int fn_device_view(fn_ctx* c, int field, fn_view* out) {
 
 FN_API int fn_download(fn_ctx* c, int field, double* host) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_download");
     int r = check_ready(c);
     if (r) return r;
     if (!host) return fail(c, FN_ERR_ARG, "fn_download: null host pointer");
@@ -1691,6 +1695,7 @@ int energy_async(fn_ctx* c, int net, double* out) {
 
 FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_observe");
     int r = check_ready(c);
     if (r) return r;
     if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_observe: bad arguments");
@@ -1710,6 +1715,7 @@ FN_API int fn_observe(fn_ctx* c, int net, int reaction_type, fn_observables* out
 
 FN_API int fn_energy_eval(fn_ctx* c, int net, fn_energy* out) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_energy_eval");
     int r = check_ready(c);
     if (r) return r;
     if (!out || net < 0 || net >= c->n_nets) return fail(c, FN_ERR_ARG, "fn_energy_eval: bad arguments");
@@ -1734,6 +1740,7 @@ FN_API int fn_energy_eval(fn_ctx* c, int net, fn_energy* out) {
 FN_API int fn_step_series(fn_ctx* c, int nsteps, int every, int net, int reaction_type,
                           int with_energy, double* host_rows) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_step_series");
     int r = check_ready(c);
     if (r) return r;
     if (nsteps <= 0 || every <= 0 || net < 0 || net >= c->n_nets || !host_rows)
@@ -1903,6 +1910,7 @@ FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, doubl
    size is kept. */
 FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_autotune");
     int r = check_ready(c);
     if (r) return r;
     if (steps_per_trial <= 0) return fail(c, FN_ERR_ARG, "fn_autotune: steps_per_trial must be positive");

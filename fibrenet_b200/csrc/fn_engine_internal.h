@@ -16,6 +16,8 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fibrenet.h"
 #include "fn_kernels.h"
 #include "fn_types.h"
@@ -141,6 +143,17 @@ struct fn_ctx {
 namespace fnh {
 
 int fail(fn_ctx* c, int code, const std::string& msg);
+
+/* Named NVTX range over a host-side phase (upload, a RunSimulationLoop call,
+   a contact rebuild, a download, ...): a profiler groups the kernels launched
+   inside it by that name (ncu --nvtx --nvtx-include "fn_rebuild/"); without a
+   profiler attached a push/pop costs a few nanoseconds. */
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 /* Entry points of the C ABI wrap their bodies in FN_TRY ... FN_CATCH(ctx) so
    that no C++ exception (host memory or threads running out) crosses the
