@@ -1,0 +1,57 @@
+/*
+ * harness.cu -- TEST INFRASTRUCTURE ONLY.
+ *
+ * The library's host engine (fn_engine.cu) built against the host stand-ins
+ * of fake_cuda.h, with the kernel launchers stubbed, so that fn_create +
+ * fn_upload run to completion on a machine without a GPU.  The hu_* entry
+ * points expose what the upload staged (bead order, packed bead arrays,
+ * spring ends, the bond path chosen) to tests/test_upload_host.py.
+ */
+#include "../../fibrenet_b200/csrc/fn_engine.cu"
+
+namespace fn {
+/* no kernel runs here: every launcher reports success and does nothing */
+cudaError_t launch_energy(const EnergyArgs&, int, double*, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_export_xyz(const double4*, const int*, int, double*, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_export_xyz(const float4*, const int*, int, double*, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_step(const StepArgs&, int, int, bool, bool, bool, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_step_tiled(const StepArgs&, int, int, bool, bool, bool, cudaStream_t) { return cudaSuccess; }
+cudaError_t prepare_step_tiled(size_t) { return cudaSuccess; }
+cudaError_t launch_step_chain(const StepArgs&, int, int, bool, bool, bool, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_forces_chain(const StepArgs&, int, int, int, cudaStream_t) { return cudaSuccess; }
+cudaError_t prepare_step_chain(size_t) { return cudaSuccess; }
+cudaError_t launch_drift(const StepArgs&, int, int, bool, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_forces_only(const StepArgs&, int, int, int, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_reset_energy(float4*, float4*, float4*, int, cudaStream_t) { return cudaSuccess; }
+long long scan_block_count(long long n) { return (n + 2047) / 2048; }
+cudaError_t launch_rebuild(const RebuildArgs&, int, int, int, long long, int*, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_observe(const ObserveArgs&, int, double*, cudaStream_t) { return cudaSuccess; }
+cudaError_t launch_verlet_rebuild(const RebuildArgs&, const FnTile*, const double4*, double4*, double, int*, int,
+                                  int, int, long long, int*, cudaStream_t) {
+    return cudaSuccess;
+}
+}  // namespace fn
+
+namespace fnh {
+/* the adjoint state is never created here */
+void adjoint_free(fn_ctx*) {}
+}  // namespace fnh
+
+#define HU_API extern "C" __attribute__((visibility("default")))
+
+HU_API int hu_create(int reorder, int chain_mode, fn_ctx** out) {
+    fn_config cfg = {0, 64, 64, reorder, 0, 128, chain_mode, 0.0};
+    return fn_create(&cfg, out);
+}
+HU_API int hu_upload(fn_ctx* c, int n, const fn_network_desc* d) { return fn_upload(c, n, d); }
+HU_API const char* hu_error(fn_ctx* c) { return fn_last_error(c); }
+HU_API int hu_permutation(fn_ctx* c, int* perm) { return fn_get_permutation(c, perm); }
+HU_API int hu_chain(fn_ctx* c) { return c->chain ? 1 : 0; }
+/* packed bead arrays in internal order: position (.w radius/type) and image (.w 1/mass) */
+HU_API void hu_beads(fn_ctx* c, double* pos4, double* img4) {
+    std::memcpy(pos4, c->pos[0].p, sizeof(double4) * c->nb);
+    std::memcpy(img4, c->img[0].p, sizeof(double4) * c->nb);
+}
+/* spring ends in internal numbering, as the device holds them */
+HU_API void hu_springs(fn_ctx* c, int* ends) { std::memcpy(ends, c->sp_ends.p, sizeof(int2) * c->ns); }
+HU_API void hu_destroy(fn_ctx* c) { fn_destroy(c); }

@@ -1,0 +1,217 @@
+"""The model upload's host logic on the CPU: fn_create + fn_upload built
+against host stand-ins for the CUDA runtime (tests/host_upload/), so the bead
+ordering, the packed bead arrays, the spring ends, the bond path chosen and
+the argument checks are checked without a GPU.  The rule the order must
+follow is restated here: spring-connected components (fibres) sorted by the
+Morton code of their lowest bead (then that bead's index), the beads of each
+component in file order."""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+HERE = os.path.join(ROOT, "tests", "host_upload")
+LIB = os.path.join(HERE, "_build", "libhostupload.so")
+SOURCES = [os.path.join(HERE, "harness.cu"), os.path.join(HERE, "fake_cuda.h")] + [
+    os.path.join(ROOT, "fibrenet_b200", "csrc", f)
+    for f in ("fn_engine.cu", "fn_engine_internal.h", "fn_kernels.h", "fn_types.h")] + [
+    os.path.join(ROOT, "include", "fibrenet.h")]
+
+
+@pytest.fixture(scope="module")
+def hu():
+    from fibrenet_b200 import build
+    if not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in SOURCES):
+        os.makedirs(os.path.dirname(LIB), exist_ok=True)
+        cmd = [build.nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O1",
+               "-Xcompiler", "-fPIC", "-include", os.path.join(HERE, "fake_cuda.h"), "-shared",
+               "-o", LIB + ".tmp", os.path.join(HERE, "harness.cu")]
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        if out.returncode != 0:
+            pytest.fail("building the host upload harness failed:\n" + out.stderr[-3000:])
+        os.replace(LIB + ".tmp", LIB)
+    lib = C.CDLL(LIB)
+    lib.hu_error.restype = C.c_char_p
+    lib.hu_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    for f in ("hu_upload", "hu_permutation", "hu_chain", "hu_beads", "hu_springs", "hu_destroy",
+              "hu_error"):
+        getattr(lib, f).argtypes = None
+    return lib
+
+
+class Upload:
+    def __init__(self, lib, models, reorder=True, chain=True):
+        from fibrenet_b200 import native
+        self.lib = lib
+        self.models = models if isinstance(models, list) else [models]
+        self.h = C.c_void_p()
+        assert lib.hu_create(int(reorder), 0 if chain else 2, C.byref(self.h)) == 0
+        keep = native._Keep()
+        descs = (native.FnNetworkDesc * len(self.models))(*[native.network_desc(m, keep) for m in self.models])
+        self.rc = lib.hu_upload(self.h, len(self.models), descs)
+        self.err = lib.hu_error(self.h).decode()
+        self.nb = sum(m.n_beads for m in self.models)
+        self.ns = sum(m.n_springs for m in self.models)
+
+    def perm(self):
+        p = np.zeros(self.nb, np.int32)
+        assert self.lib.hu_permutation(self.h, p.ctypes.data_as(C.c_void_p)) == 0
+        return p
+
+    def beads(self):
+        pos = np.zeros((self.nb, 4)); img = np.zeros((self.nb, 4))
+        self.lib.hu_beads(self.h, pos.ctypes.data_as(C.c_void_p), img.ctypes.data_as(C.c_void_p))
+        return pos, img
+
+    def springs(self):
+        e = np.zeros((max(self.ns, 1), 2), np.int32)
+        self.lib.hu_springs(self.h, e.ctypes.data_as(C.c_void_p))
+        return e[:self.ns]
+
+    def close(self):
+        self.lib.hu_destroy(self.h)
+
+
+def _spread10(v):
+    v = v.astype(np.uint64) & 0x3FF
+    v = (v | (v << 16)) & 0x030000FF
+    v = (v | (v << 8)) & 0x0300F00F
+    v = (v | (v << 4)) & 0x030C30C3
+    v = (v | (v << 2)) & 0x09249249
+    return v
+
+
+def expected_order(m):
+    """Internal order of one network: components by (Morton code of the
+    lowest bead, its index), beads of a component ascending."""
+    n = m.n_beads
+    parent = np.arange(n)
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+    for a, b in zip(m.s_p1, m.s_p2):
+        ra, rb = find(a), find(b)
+        if ra != rb:
+            parent[max(ra, rb)] = min(ra, rb)
+    root = np.array([find(i) for i in range(n)])
+    roots = np.unique(root)
+    x = m.pos[roots] / np.asarray(m.settings.box) * 1024.0
+    x = np.where(x >= 0.0, x, 0.0)
+    q = np.minimum(x, 1023.0).astype(np.uint32)
+    code = _spread10(q[:, 0]) | (_spread10(q[:, 1]) << 1) | (_spread10(q[:, 2]) << 2)
+    key = {int(r): (int(c), int(r)) for r, c in zip(roots, code)}
+    return np.array(sorted(range(n), key=lambda i: (key[int(root[i])], i)), np.int32)
+
+
+def small_tensile(seed=8):
+    from fibrenet_b200 import generate as g
+    return g.tensile_network(seed=seed, fibres=40, beads=20, box=(40.0, 30.0, 8.0), z_range=(1.0, 7.0),
+                             clamp_lo=2.0, clamp_hi=38.0, cell=2.5)
+
+
+def test_bead_order_and_staged_beads(hu):
+    m = small_tensile().normalised()
+    u = Upload(hu, m)
+    try:
+        assert u.rc == 0, u.err
+        perm = u.perm()
+        np.testing.assert_array_equal(perm, expected_order(m))
+        pos, img = u.beads()
+        np.testing.assert_array_equal(pos[:, :3], m.pos[perm])
+        np.testing.assert_array_equal(img[:, :3], m.img[perm])
+        minv = np.where(m.mass > 0, 1.0 / np.where(m.mass > 0, m.mass, 1.0), 0.0)
+        np.testing.assert_array_equal(img[:, 3], minv[perm])
+        inv = np.empty_like(perm)
+        inv[perm] = np.arange(len(perm))
+        np.testing.assert_array_equal(u.springs(), np.stack([inv[m.s_p1], inv[m.s_p2]], 1))
+        assert hu.hu_chain(u.h) == 1
+    finally:
+        u.close()
+
+
+def test_general_topology_order_and_bond_path(hu):
+    from test_gpu_parity import _crosslinked
+    m = _crosslinked().normalised()
+    u = Upload(hu, m)
+    try:
+        assert u.rc == 0, u.err
+        np.testing.assert_array_equal(u.perm(), expected_order(m))
+        assert hu.hu_chain(u.h) == 0  # cross-links: not chain form
+    finally:
+        u.close()
+
+
+def test_reversed_and_shuffled_springs(hu):
+    from test_gpu_parity import _reversed
+    m = _reversed(small_tensile(9))
+    u = Upload(hu, m)
+    try:
+        assert u.rc == 0, u.err
+        np.testing.assert_array_equal(u.perm(), expected_order(m))
+        assert hu.hu_chain(u.h) == 1
+    finally:
+        u.close()
+    m = small_tensile(10).normalised().copy()
+    p = np.random.default_rng(3).permutation(m.n_springs)
+    for f in ("s_type", "s_tag", "s_p1", "s_p2", "s_rest", "s_k", "s_c1", "s_c2"):
+        setattr(m, f, getattr(m, f)[p].copy())
+    u = Upload(hu, m)
+    try:
+        assert u.rc == 0, u.err
+        np.testing.assert_array_equal(u.perm(), expected_order(m))
+        assert hu.hu_chain(u.h) == 0  # bonds out of ascending order around a bead
+    finally:
+        u.close()
+
+
+def test_file_order_kept_without_reorder(hu):
+    m = small_tensile(11).normalised()
+    u = Upload(hu, m, reorder=False)
+    try:
+        assert u.rc == 0, u.err
+        np.testing.assert_array_equal(u.perm(), np.arange(m.n_beads))
+    finally:
+        u.close()
+
+
+def test_batch_orders_each_network_in_its_range(hu):
+    from fibrenet_b200 import generate as g
+    models = [m.normalised() for m in g.ensemble_networks(seed=3, n_networks=3, fibres_lo=5, fibres_hi=30)]
+    u = Upload(hu, models)
+    try:
+        assert u.rc == 0, u.err
+        perm = u.perm()
+        base = 0
+        for m in models:
+            np.testing.assert_array_equal(perm[base:base + m.n_beads] - base, expected_order(m))
+            base += m.n_beads
+    finally:
+        u.close()
+
+
+@pytest.mark.parametrize("field,idx,val,msg", [
+    ("type", 37, 9, "bead 37 has an undeclared type"),
+    ("mass", 40, -1.0, "negative mass"),
+    ("s_p2", 55, 10**6, "spring 55 references a missing bead"),
+    ("a_b3", 70, -2, "angle 70 references a missing bead"),
+])
+def test_invalid_models_are_named(hu, field, idx, val, msg):
+    m = small_tensile(12).normalised().copy()
+    a = getattr(m, field).copy()
+    a[idx] = val
+    a[idx + 5] = val  # a later offender too: the first one is reported
+    setattr(m, field, a)
+    u = Upload(hu, m)
+    try:
+        assert u.rc == 1
+        assert msg in u.err, u.err
+    finally:
+        u.close()
