@@ -54,4 +54,20 @@ HU_API void hu_beads(fn_ctx* c, double* pos4, double* img4) {
 }
 /* spring ends in internal numbering, as the device holds them */
 HU_API void hu_springs(fn_ctx* c, int* ends) { std::memcpy(ends, c->sp_ends.p, sizeof(int2) * c->ns); }
+/* the tile table every launch reads: (network, first bead, end bead) */
+HU_API int hu_tiles(fn_ctx* c, int* out3, int cap) {
+    for (int t = 0; t < c->ntiles && t < cap; ++t) {
+        const FnTile& x = c->tiles.p[t];
+        out3[3 * t] = x.net;
+        out3[3 * t + 1] = x.begin;
+        out3[3 * t + 2] = x.end;
+    }
+    return c->ntiles;
+}
+HU_API int hu_block(fn_ctx* c) { return c->block; }
+/* bead -> spring incidence (CSR, internal numbering; entry = spring << 1 | end) */
+HU_API void hu_spring_incidence(fn_ctx* c, int* off, int* ent) {
+    std::memcpy(off, c->sp_off_h.data(), sizeof(int) * c->sp_off_h.size());
+    std::memcpy(ent, c->sp_ent_h.data(), sizeof(int) * c->sp_ent_h.size());
+}
 HU_API void hu_destroy(fn_ctx* c) { fn_destroy(c); }

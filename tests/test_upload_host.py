@@ -39,7 +39,7 @@ def hu():
     lib.hu_error.restype = C.c_char_p
     lib.hu_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
     for f in ("hu_upload", "hu_permutation", "hu_chain", "hu_beads", "hu_springs", "hu_destroy",
-              "hu_error"):
+              "hu_error", "hu_tiles", "hu_block", "hu_spring_incidence"):
         getattr(lib, f).argtypes = None
     return lib
 
@@ -213,5 +213,59 @@ def test_invalid_models_are_named(hu, field, idx, val, msg):
     try:
         assert u.rc == 1
         assert msg in u.err, u.err
+    finally:
+        u.close()
+
+
+def _tiles(hu, u):
+    cap = u.nb + 1
+    t = np.zeros((cap, 3), np.int32)
+    n = hu.hu_tiles(u.h, t.ctypes.data_as(C.c_void_p), cap)
+    return t[:n]
+
+
+def test_tiles_cover_each_network_without_crossing_it(hu):
+    """The tile table drives every launch of a batch: each block's beads lie
+    in one network, every bead is in exactly one tile, and a chain tile holds
+    block - 4 beads (its two-bead halo on each side fills the block)."""
+    from fibrenet_b200 import generate as g
+    models = [m.normalised() for m in g.ensemble_networks(seed=4, n_networks=4, fibres_lo=3, fibres_hi=25)]
+    u = Upload(hu, models)
+    try:
+        assert u.rc == 0, u.err
+        tiles = _tiles(hu, u)
+        block = hu.hu_block(u.h)
+        starts = np.cumsum([0] + [m.n_beads for m in models])
+        covered = np.zeros(u.nb, np.int32)
+        for net, b, e in tiles:
+            assert starts[net] <= b < e <= starts[net + 1]
+            assert e - b <= block - 4
+            covered[b:e] += 1
+        np.testing.assert_array_equal(covered, 1)
+    finally:
+        u.close()
+
+
+def test_spring_incidence_lists_every_end_in_order(hu):
+    """General topology (cross-links): each bead lists its springs in
+    ascending index, each spring appears once at each of its two ends."""
+    from test_gpu_parity import _crosslinked
+    m = _crosslinked().normalised()
+    u = Upload(hu, m, chain=False)
+    try:
+        assert u.rc == 0, u.err
+        off = np.zeros(u.nb + 1, np.int32)
+        ent = np.zeros(2 * u.ns, np.int32)
+        hu.hu_spring_incidence(u.h, off.ctypes.data_as(C.c_void_p), ent.ctypes.data_as(C.c_void_p))
+        ends = u.springs()
+        seen = np.zeros((u.ns, 2), np.int32)
+        for i in range(u.nb):
+            row = ent[off[i]:off[i + 1]]
+            assert np.all(np.diff(row >> 1) >= 0)
+            for x in row:
+                s_, end = x >> 1, x & 1
+                assert ends[s_, end] == i
+                seen[s_, end] += 1
+        np.testing.assert_array_equal(seen, 1)
     finally:
         u.close()
