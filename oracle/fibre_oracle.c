@@ -857,6 +857,25 @@ FO_EXPORT void fo_get_lists(const fo_ctx* c, int* head, int* partners, int* pair
 
 FO_EXPORT double fo_detmath_acos(double x) { return fn_acos(x); }
 
+/* The settings derived from the input (SimulationManager.cpp:647-720,
+   804-805, 2178-2190) as 20 doubles: dt, half_dt, half_dt2, lambda_dt,
+   damping, cutoff_sq, wall_k, gravity[3], box[3], step[3], half_box_sq, nx,
+   ny, nz; and the pair table (SimulationManager.cpp:859-942): 6 coefficients
+   and the kind per pair.  For checks of a host precompute against this one. */
+FO_EXPORT void fo_get_derived(const fo_ctx* c, double* out20) {
+    const fo_derived* d = &c->d;
+    const double v[20] = {d->dt, d->half_dt, d->half_dt2, d->lambda_dt, d->damping, d->cutoff_sq, d->wall_k,
+                          d->gravity[0], d->gravity[1], d->gravity[2], d->box[0], d->box[1], d->box[2],
+                          d->step[0], d->step[1], d->step[2], d->half_box_sq, (double)d->nx, (double)d->ny,
+                          (double)d->nz};
+    memcpy(out20, v, sizeof v);
+}
+FO_EXPORT int fo_get_pairs(const fo_ctx* c, double* coeffs6, int* kinds) {
+    memcpy(coeffs6, c->p_c, sizeof(double) * 6 * (size_t)c->np);
+    memcpy(kinds, c->p_kind, sizeof(int) * (size_t)c->np);
+    return c->np;
+}
+
 FO_EXPORT void fo_overflow(const fo_ctx* c, long* out2) {
     out2[0] = c->overflow_cells;
     out2[1] = c->overflow_lists;

@@ -145,6 +145,9 @@ def _load_oracle():
         lib.fo_get_cells.argtypes = [_P, _I, _I]
         lib.fo_get_lists.argtypes = [_P, _I, _I, _I]
         lib.fo_overflow.argtypes = [_P, C.POINTER(C.c_long)]
+        lib.fo_get_derived.argtypes = [_P, _D]
+        lib.fo_get_pairs.argtypes = [_P, _D, _I]
+        lib.fo_get_pairs.restype = C.c_int
         _oracle_lib = lib
     return _oracle_lib
 
@@ -204,6 +207,20 @@ class OracleSim(_Base):
 
     def run(self, n: int):
         assert self.lib.fo_run(self.h, n) == 0
+
+    def derived(self) -> np.ndarray:
+        """dt, half_dt, half_dt2, lambda_dt, damping, cutoff_sq, wall_k,
+        gravity[3], box[3], step[3], half_box_sq, nx, ny, nz."""
+        out = np.zeros(20)
+        self.lib.fo_get_derived(self.h, out.ctypes.data_as(_D))
+        return out
+
+    def pairs(self):
+        """Pair table: (coefficients c1..c6 per pair, kind per pair)."""
+        n = 64 * 65 // 2
+        c6 = np.zeros((n, 6)); k = np.zeros(n, np.int32)
+        np_ = self.lib.fo_get_pairs(self.h, c6.ctypes.data_as(_D), k.ctypes.data_as(_I))
+        return c6[:np_], k[:np_]
 
     def rebuild(self):
         self.lib.fo_rebuild(self.h)

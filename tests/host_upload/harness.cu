@@ -70,4 +70,22 @@ HU_API void hu_spring_incidence(fn_ctx* c, int* off, int* ent) {
     std::memcpy(off, c->sp_off_h.data(), sizeof(int) * c->sp_off_h.size());
     std::memcpy(ent, c->sp_ent_h.data(), sizeof(int) * c->sp_ent_h.size());
 }
+/* network k's derived settings in the oracle's fo_get_derived layout */
+HU_API void hu_net(fn_ctx* c, int k, double* out20) {
+    const FnNet& N = c->nets_h[k];
+    const double v[20] = {N.dt, N.half_dt, N.half_dt2, N.lambda_dt, N.damping, N.cutoff_sq, N.wall_k,
+                          N.g[0], N.g[1], N.g[2], N.box[0], N.box[1], N.box[2],
+                          N.step[0], N.step[1], N.step[2], N.half_box_sq, (double)N.nx, (double)N.ny,
+                          (double)N.nz};
+    std::memcpy(out20, v, sizeof v);
+}
+/* network k's pair table: 6 coefficients and the kind per pair */
+HU_API int hu_pairs(fn_ctx* c, int k, double* coeffs6, int* kinds) {
+    const int base = c->nets_h[k].pair_base, nt = c->nets_h[k].types_num, np = nt * (nt + 1) / 2;
+    for (int p = 0; p < np; ++p) {
+        std::memcpy(coeffs6 + 6 * p, c->pairs_h[base + p].c, sizeof(double) * 6);
+        kinds[p] = c->pairs_h[base + p].kind;
+    }
+    return np;
+}
 HU_API void hu_destroy(fn_ctx* c) { fn_destroy(c); }

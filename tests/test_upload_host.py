@@ -39,7 +39,7 @@ def hu():
     lib.hu_error.restype = C.c_char_p
     lib.hu_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
     for f in ("hu_upload", "hu_permutation", "hu_chain", "hu_beads", "hu_springs", "hu_destroy",
-              "hu_error", "hu_tiles", "hu_block", "hu_spring_incidence"):
+              "hu_error", "hu_tiles", "hu_block", "hu_spring_incidence", "hu_net", "hu_pairs"):
         getattr(lib, f).argtypes = None
     return lib
 
@@ -269,3 +269,51 @@ def test_spring_incidence_lists_every_end_in_order(hu):
         np.testing.assert_array_equal(seen, 1)
     finally:
         u.close()
+
+
+@pytest.mark.parametrize("which", ["tensile", "plain", "multitype", "dense"])
+def test_derived_settings_and_pair_table_match_the_oracle(hu, oracle_built, which):
+    """The engine's host precompute -- time-step constants, damping sign,
+    cut-off, grid size and cell step, half box, the pair coefficients (LJ
+    force shift, st remap) -- equals the oracle's restatement of
+    SimulationManager's, bit for bit."""
+    import pyoracle as po
+    from fibrenet_b200 import generate as g
+    if which == "tensile":
+        m = small_tensile(13)
+    elif which == "plain":
+        m = g.plain_network(seed=1, fibres=20, beads=10, box=(20.0, 20.0, 6.0), z_range=(1.0, 5.0))
+    elif which == "dense":
+        m = g.dense_mat(seed=2, fibres=40, beads=10, box=(12.0, 12.0, 12.0))
+    else:
+        m = _multitype()
+    m = m.normalised()
+    u = Upload(hu, m)
+    try:
+        assert u.rc == 0, u.err
+        mine = np.zeros(20)
+        hu.hu_net(u.h, 0, mine.ctypes.data_as(C.c_void_p))
+        c6 = np.zeros((m.n_types * (m.n_types + 1) // 2, 6)); kinds = np.zeros(len(c6), np.int32)
+        hu.hu_pairs(u.h, 0, c6.ctypes.data_as(C.c_void_p), kinds.ctypes.data_as(C.c_void_p))
+    finally:
+        u.close()
+    o = po.OracleSim(m, po.MODE_REF)
+    np.testing.assert_array_equal(mine, o.derived())
+    oc6, okinds = o.pairs()
+    np.testing.assert_array_equal(kinds, okinds)
+    np.testing.assert_array_equal(c6, oc6)
+
+
+def _multitype():
+    """Three bead types with one lj, one hs and one st pair among them."""
+    from fibrenet_b200 import generate as g
+    from fibrenet_b200.model import PAIR_HS, PAIR_LJ, PAIR_ST
+    m = g.plain_network(seed=3, fibres=12, beads=8, box=(16.0, 16.0, 6.0), z_range=(1.0, 5.0)).normalised().copy()
+    m.type = (np.arange(m.n_beads) % 3).astype(np.int32)
+    m.type_names = ["A", "B", "C"]
+    kinds = [PAIR_LJ, PAIR_HS, PAIR_ST, PAIR_LJ, PAIR_HS, PAIR_ST]
+    raw = [[1.0, 1.0, 2.5, 0.0], [50.0, 0.0, 0.0, 0.0], [1.0, 20.0, 1.5, 5.0],
+           [0.9, 0.5, 2.2, 0.0], [30.0, 0.0, 0.0, 0.0], [0.8, 10.0, 1.2, 3.0]]
+    m.pair_kind = np.array(kinds, np.int32)
+    m.pair_raw = np.array(raw, np.float64).reshape(-1)
+    return m
