@@ -88,4 +88,10 @@ HU_API int hu_pairs(fn_ctx* c, int k, double* coeffs6, int* kinds) {
     }
     return np;
 }
+/* chain-form records per bead (internal order): next spring rest, k, c1, c2
+   and centred angle theta0, k */
+HU_API void hu_chain_records(fn_ctx* c, float* sp4, float* an2) {
+    std::memcpy(sp4, c->ch_sp.p, sizeof(float4) * c->nb);
+    std::memcpy(an2, c->ch_an.p, sizeof(float2) * c->nb);
+}
 HU_API void hu_destroy(fn_ctx* c) { fn_destroy(c); }

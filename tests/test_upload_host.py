@@ -39,7 +39,8 @@ def hu():
     lib.hu_error.restype = C.c_char_p
     lib.hu_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
     for f in ("hu_upload", "hu_permutation", "hu_chain", "hu_beads", "hu_springs", "hu_destroy",
-              "hu_error", "hu_tiles", "hu_block", "hu_spring_incidence", "hu_net", "hu_pairs"):
+              "hu_error", "hu_tiles", "hu_block", "hu_spring_incidence", "hu_net", "hu_pairs",
+              "hu_chain_records", "fn_set_springs", "fn_set_angles", "fn_set_mass"):
         getattr(lib, f).argtypes = None
     return lib
 
@@ -317,3 +318,43 @@ def _multitype():
     m.pair_kind = np.array(kinds, np.int32)
     m.pair_raw = np.array(raw, np.float64).reshape(-1)
     return m
+
+
+def test_modifications_reach_the_chain_records(hu):
+    """fn_set_springs / fn_set_angles / fn_set_mass (the reference's
+    modif_spring and modif_bead, SimulationManager.cpp:189-636): values given
+    in file order land on the right beads of the chain records and of the
+    image positions' 1/mass."""
+    m = small_tensile(14).normalised()
+    u = Upload(hu, m)
+    try:
+        assert u.rc == 0, u.err
+        rng = np.random.default_rng(5)
+        rest = rng.uniform(0.5, 1.5, m.n_springs)
+        k = rng.uniform(10, 200, m.n_springs)
+        theta0 = rng.uniform(2.5, 3.1, m.n_angles)
+        ka = rng.uniform(1, 20, m.n_angles)
+        mass = rng.uniform(0.5, 2.0, m.n_beads)
+        mass[::7] = 0.0
+        P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        assert hu.fn_set_springs(u.h, P(rest), P(k), None, None) == 0
+        assert hu.fn_set_angles(u.h, P(theta0), P(ka)) == 0
+        assert hu.fn_set_mass(u.h, P(mass)) == 0
+        sp4 = np.zeros((u.nb, 4), np.float32)
+        an2 = np.zeros((u.nb, 2), np.float32)
+        hu.hu_chain_records(u.h, P(sp4), P(an2))
+        perm = u.perm()
+        inv = np.empty_like(perm)
+        inv[perm] = np.arange(len(perm))
+        lower = np.minimum(inv[m.s_p1], inv[m.s_p2])
+        np.testing.assert_array_equal(sp4[lower, 0], rest.astype(np.float32))
+        np.testing.assert_array_equal(sp4[lower, 1], k.astype(np.float32))
+        np.testing.assert_array_equal(sp4[lower, 2], m.s_c1.astype(np.float32))
+        centre = inv[m.a_b2]
+        np.testing.assert_array_equal(an2[centre, 0], theta0.astype(np.float32))
+        np.testing.assert_array_equal(an2[centre, 1], ka.astype(np.float32))
+        _, img = u.beads()
+        want = np.where(mass > 0, 1.0 / np.where(mass > 0, mass, 1.0), 0.0)
+        np.testing.assert_array_equal(img[:, 3], want[perm])
+    finally:
+        u.close()
