@@ -40,7 +40,8 @@ def hu():
     lib.hu_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p)]
     for f in ("hu_upload", "hu_permutation", "hu_chain", "hu_beads", "hu_springs", "hu_destroy",
               "hu_error", "hu_tiles", "hu_block", "hu_spring_incidence", "hu_net", "hu_pairs",
-              "hu_chain_records", "fn_set_springs", "fn_set_angles", "fn_set_mass"):
+              "hu_chain_records", "fn_set_springs", "fn_set_angles", "fn_set_mass",
+              "fn_set_status", "fn_download_status"):
         getattr(lib, f).argtypes = None
     return lib
 
@@ -356,5 +357,31 @@ def test_modifications_reach_the_chain_records(hu):
         _, img = u.beads()
         want = np.where(mass > 0, 1.0 / np.where(mass > 0, mass, 1.0), 0.0)
         np.testing.assert_array_equal(img[:, 3], want[perm])
+    finally:
+        u.close()
+
+
+@pytest.mark.parametrize("chain", [True, False])
+def test_status_round_trip(hu, chain):
+    """Spring and angle statuses set in file order come back unchanged, both
+    from the chain form's per-bead status bits and from the per-bond arrays
+    of the incidence path; every upload starts with all bonds alive."""
+    m = small_tensile(15).normalised()
+    u = Upload(hu, m, chain=chain)
+    try:
+        assert u.rc == 0, u.err
+        assert hu.hu_chain(u.h) == int(chain)
+        P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        s0 = np.zeros(m.n_springs, np.int32); a0 = np.zeros(m.n_angles, np.int32)
+        assert hu.fn_download_status(u.h, P(s0), P(a0)) == 0
+        assert s0.all() and a0.all()
+        rng = np.random.default_rng(6)
+        s1 = (rng.random(m.n_springs) < 0.7).astype(np.int32)
+        a1 = (rng.random(m.n_angles) < 0.6).astype(np.int32)
+        assert hu.fn_set_status(u.h, P(s1), P(a1)) == 0
+        s2 = np.zeros_like(s1); a2 = np.zeros_like(a1)
+        assert hu.fn_download_status(u.h, P(s2), P(a2)) == 0
+        np.testing.assert_array_equal(s2, s1)
+        np.testing.assert_array_equal(a2, a1)
     finally:
         u.close()
