@@ -8,6 +8,7 @@
  * step kernels on one stream (RunSimulationLoop, SimulationManager.cpp:151-181).
  */
 #include <cuda_runtime.h>
+#include <sched.h>
 
 #include <algorithm>
 #include <atomic>
@@ -75,12 +76,24 @@ struct HostArray {
     const T& operator[](size_t i) const { return p[i]; }
 };
 
+/* Host threads this process may run on: its CPU affinity mask (what a
+   container's cpuset allows), else the machine's count. */
+long long host_threads() {
+    static const long long n = [] {
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        if (sched_getaffinity(0, sizeof set, &set) == 0 && CPU_COUNT(&set) > 0) return (long long)CPU_COUNT(&set);
+        return (long long)std::max(1u, std::thread::hardware_concurrency());
+    }();
+    return n;
+}
+
 /* Runs f(begin, end) over [0, n) on up to 32 host threads (the upload's
    conversions are independent per element). */
 template <class F>
 void parallel_for(long long n, F f) {
     const long long min_chunk = 1 << 15;
-    long long nt = std::min<long long>(32, std::max(1u, std::thread::hardware_concurrency()));
+    long long nt = std::min<long long>(32, host_threads());
     nt = std::max(1LL, std::min(nt, (n + min_chunk - 1) / min_chunk));
     if (nt <= 1) {
         f(0LL, n);
