@@ -6,13 +6,21 @@ finite box 1000x1000x20 with x and z walls and periodic y, HR_FL springs with
 E = 1e3 and lognormal failure stress, HR angles, LJ contacts with cut-off
 2.5, clamps at x < 2 and x > 998, dt = 0.0005), generated from a fixed seed
 because the reference ships no models.  One bench step is one time step of
-RunSimulationLoop over all beads; the contact list is rebuilt every 8 steps
-as in the reference.
+RunSimulationLoop over all beads; the contact list is rebuilt at step 0 of
+every call and every 8 steps, as in the reference.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The timed region is fn_step(K) from one saved state, repeated (the state
+restored between repetitions, outside the events) until about a second of
+device time has been measured; the line reports the median repetition.
+At N = 1 the line also carries the other parts of the task's metric as
+sub-objects: the batched ensemble against the same networks one by one, the
+adjoint sweep against the forward pass, the dense mat and the small
+network.
+
 --impl reference times the reference's own kernels (FibreNet/kernel.cl compiled
-as C, oracle/_ref) on the host cores for the same workload and metric.
+as C, oracle/_ref) on the host cores for the same workload, the same K and W.
 With N > 1 (torchrun) every rank runs an independent replica: the path is one
 network and does not shard ("replicas only"); value = all ranks' bead-steps
 over the slowest rank's device time.
@@ -21,6 +29,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -34,18 +43,23 @@ METRIC = "bead-steps/s (tensile network, 1 B200 per replica)"
 UNIT = "bead-steps/s"
 WORKLOAD = "tensile_1M"
 OUTPUT_FREQ = 100  # the tensile test records reaction force / broken springs every 100 steps
+REBUILD_KERNELS = 7  # k_cells, three scan kernels, k_scatter, k_cell_sort, k_lists
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=2000)
-    p.add_argument("--warmup", type=int, default=40)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--fibres", type=int, default=None,
                    help="fibre count (default 20,000 tensile / 40,000 dense)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the ensemble / adjoint / dense / small-network sub-results")
+    p.add_argument("--min-ms", type=float, default=1000.0,
+                   help="device time the repeated timed region covers at least")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--workload", choices=["tensile", "dense", "ensemble", "adjoint", "plain"],
                    default="tensile",
@@ -66,17 +80,30 @@ def parse():
     return a
 
 
+def tensile_model(fibres: int = 20000):
+    """The tensile network, placed by the numpy generator (no native code), so
+    that both arms of the bench build the same model without loading the
+    library under test."""
+    from fibrenet_b200 import generate as g
+    s = (fibres / 20000.0) ** 0.5
+    box = (1000.0 * s, 1000.0 * s, 20.0)
+    return g.tensile_network(seed=1, fibres=fibres, beads=50, box=box, clamp_lo=2.0,
+                             clamp_hi=box[0] - 2.0, placement="host")
+
+
+def dense_model(fibres: int = 40000):
+    from fibrenet_b200 import generate as g
+    s = (fibres / 40000.0) ** (1.0 / 3.0)
+    return g.dense_mat(seed=2, fibres=fibres, beads=100, box=(200.0 * s,) * 3)
+
+
 def workload(args):
     from fibrenet_b200 import generate as g
     if args.workload == "plain":
         return g.plain_network(seed=0)
     if args.workload == "dense":
-        s = (args.fibres / 40000.0) ** (1.0 / 3.0)
-        return g.dense_mat(seed=2, fibres=args.fibres, beads=100, box=(200.0 * s,) * 3)
-    s = (args.fibres / 20000.0) ** 0.5
-    box = (1000.0 * s, 1000.0 * s, 20.0)
-    return g.tensile_network(seed=1, fibres=args.fibres, beads=50, box=box, clamp_lo=2.0,
-                             clamp_hi=box[0] - 2.0)
+        return dense_model(args.fibres)
+    return tensile_model(args.fibres)
 
 
 def metric_for(args):
@@ -87,35 +114,32 @@ def metric_for(args):
     return METRIC
 
 
-def config_dict(m, args, extra=None):
-    if args.workload == "plain":
+def config_dict(m, args, extra=None, workload_name=None):
+    wl = workload_name or args.workload
+    if wl == "plain":
         d = {"workload": "plain_10k", "beads": m.n_beads, "fibres": 200, "beads_per_fibre": 50,
              "box": list(m.settings.box), "contacts": "penalty k 50", "dt": m.settings.dt,
              "grid_update_freq": m.settings.grid_update_freq}
-        if extra:
-            d.update(extra)
-        return d
-    if args.workload == "dense":
-        name = "dense_4M" if args.fibres == 40000 else f"dense_{m.n_beads}"
-        d = {"workload": name, "beads": m.n_beads, "springs": m.n_springs, "angles": m.n_angles,
-             "fibres": args.fibres, "beads_per_fibre": 100, "box": list(m.settings.box),
-             "bc": "periodic x,y,z",
+    elif wl == "dense":
+        fib = m.n_beads // 100
+        d = {"workload": "dense_4M" if fib == 40000 else f"dense_{m.n_beads}", "beads": m.n_beads,
+             "springs": m.n_springs, "angles": m.n_angles, "fibres": fib, "beads_per_fibre": 100,
+             "box": list(m.settings.box), "bc": "periodic x,y,z",
              "contacts": "penalty k 100 on overlap + soft harmonic k 10 below 1.2 (pair kind hsr)",
              "dt": m.settings.dt, "grid_update_freq": m.settings.grid_update_freq,
              "cell": m.settings.box_unit_cell, "seed": 2,
-             "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single",
              "l2": "working set above 126 MB L2 (inputs larger than L2, no flush)"}
-        if extra:
-            d.update(extra)
-        return d
-    d = {"workload": WORKLOAD if args.fibres == 20000 else f"tensile_{m.n_beads}",
-         "beads": m.n_beads, "springs": m.n_springs, "angles": m.n_angles,
-         "fibres": args.fibres, "beads_per_fibre": 50, "box": list(m.settings.box),
-         "bc": "finite x,z / periodic y", "contacts": "LJ eps 1 sigma 1 cut 2.5",
-         "dt": m.settings.dt, "grid_update_freq": m.settings.grid_update_freq,
-         "cell": m.settings.box_unit_cell, "seed": 1,
-         "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single",
-         "l2": "working set above 126 MB L2 (inputs larger than L2, no flush)"}
+    else:
+        fib = m.n_beads // 50
+        d = {"workload": WORKLOAD if fib == 20000 else f"tensile_{m.n_beads}",
+             "beads": m.n_beads, "springs": m.n_springs, "angles": m.n_angles,
+             "fibres": fib, "beads_per_fibre": 50, "box": list(m.settings.box),
+             "bc": "finite x,z / periodic y", "contacts": "LJ eps 1 sigma 1 cut 2.5",
+             "dt": m.settings.dt, "grid_update_freq": m.settings.grid_update_freq,
+             "cell": m.settings.box_unit_cell, "seed": 1, "placement": "numpy generator, min separation 1.0",
+             "l2": "working set above 126 MB L2 (inputs larger than L2, no flush)"}
+    if args is not None:
+        d["parallelism"] = f"replicas{args.gpus}" if args.gpus > 1 else "single"
     if extra:
         d.update(extra)
     return d
@@ -149,6 +173,7 @@ class ClockSampler:
             if self.path:
                 self.f.close()
                 os.remove(self.path)
+        return self
 
     def stop(self):
         if self.proc is None:
@@ -221,11 +246,18 @@ def traffic_from_profiles():
     return None
 
 
+def rebuilds_per_call(K: int, freq: int) -> int:
+    """Contact rebuilds of one fn_step(K) call: at step 0 and every freq steps
+    (the counter restarts with every call, SimulationManager.cpp:152)."""
+    return -(-K // freq)
+
+
 def cpu_reference_rate(model, seconds: float, threads: int | None = None, steps_cap: int = 10**9,
-                       warmup: int = 1):
+                       warmup: int = 1, chunk: int = 8):
     """Reference kernels (oracle/_ref) on the host cores; a time-bounded
-    sample of whole steps.  Returns (bead-steps/s, steps, threads, kind)."""
-    threads = threads or os.cpu_count()
+    sample of whole steps in calls of `chunk` steps.  Returns (bead-steps/s,
+    steps, threads, kind)."""
+    threads = threads or len(os.sched_getaffinity(0))
     os.environ.setdefault("OMP_PROC_BIND", "true")
     os.environ.setdefault("OMP_PLACES", "cores")
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -248,13 +280,14 @@ def cpu_reference_rate(model, seconds: float, threads: int | None = None, steps_
         kind = "port"
         threads = 1
         sim = po.OracleSim(m, po.MODE_REF)
-    for _ in range(warmup):
-        sim.run(1)
+    if warmup > 0:
+        sim.run(warmup)
     done = 0
     t0 = time.perf_counter()
     while done < steps_cap:
-        sim.run(8)  # one rebuild cycle (grid_update_freq 8)
-        done += 8
+        k = min(chunk, steps_cap - done)
+        sim.run(k)
+        done += k
         if time.perf_counter() - t0 > seconds:
             break
     dt = time.perf_counter() - t0
@@ -272,81 +305,33 @@ def ref_note(args) -> dict:
 
 
 def run_reference_arm(args):
+    """The reference's own kernels (oracle/_ref, OpenMP on every host core the
+    process may use) for the same workload: W untimed steps, then exactly K
+    timed steps in one RunSimulationLoop call, as our arm's fn_step(K)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     m = workload(args)
-    budget = max(30.0, min(150.0, 3.0 * (args.steps + args.warmup)))
-    rate, done, threads, kind = cpu_reference_rate(m, budget, steps_cap=args.steps,
-                                                   warmup=min(args.warmup, 2))
+    K, W = args.steps, args.warmup
+    rate, done, threads, kind = cpu_reference_rate(m, float("inf"), steps_cap=K, warmup=W, chunk=K)
     line = {"metric": metric_for(args), "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
-            "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * m.n_beads / rate,
+            "warmup": W, "ms_per_step": 1e3 * m.n_beads / rate,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator)", "impl": "reference",
             "config": config_dict(m, args, ref_note(args)),
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{done} whole steps of the full {m.n_beads}-bead network "
-                                       f"(time-bounded, {budget:.0f} s)"},
+                             "sample": f"{done} whole steps of the full {m.n_beads}-bead network in one "
+                                       f"call after {W} warm-up steps"},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(args, m, local, dist, world, nb, barrier, block=0):
-    """Same metric through the public API with host buffers: model upload from
-    pinned host arrays, RunSimulationLoop in output_freq chunks with the
-    recorded observables read back after each chunk, final state download."""
+# --------------------------------------------------------------------------
+# our arm
+
+
+def dist_setup():
     import torch
-
-    from fibrenet_b200.native import Simulation
-
-    e2e_steps = args.steps
-    pinned = {}
-    mm = m.normalised()
-    for name in ["pos", "img", "vel", "vel_old", "force"]:
-        t = torch.from_numpy(getattr(mm, name)).pin_memory()
-        pinned[name] = t
-        setattr(mm, name, t.numpy())
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    w0 = time.perf_counter()
-    sim2 = Simulation(mm, device=local, list_capacity=64, cell_capacity=64, reorder=True,
-                      block_size=block)
-    done = 0
-    obs_bytes = 0
-    while done < e2e_steps:
-        k = min(OUTPUT_FREQ, e2e_steps - done)
-        sim2.step(k)
-        o = sim2.observe(0, reaction_type=2 if m.n_types > 2 else -1)
-        obs_bytes += 5 * 8
-        done += k
-    final = sim2.get("pos")
-    sim2.sync()
-    e1.record()
-    torch.cuda.synchronize()
-    e2e_wall = time.perf_counter() - w0
-    e2e_ms = max(e0.elapsed_time(e1), 1e3 * e2e_wall)
-    from fibrenet_b200.ranks import slowest
-    e2e_ms = slowest(e2e_ms, dist, "cuda")
-    h2d = sum(getattr(mm, k).nbytes for k in ["pos", "img", "vel", "vel_old", "force", "radius", "mass",
-                                            "type", "tag", "loc_id", "s_type", "s_p1", "s_p2",
-                                            "s_rest", "s_k", "s_c1", "s_c2", "a_type", "a_b1",
-                                            "a_b2", "a_b3", "a_s1", "a_s2", "a_theta0", "a_k"])
-    d2h = obs_bytes + final.nbytes
-    e2e_value = world * nb * e2e_steps / (e2e_ms / 1e3)
-    sim2.close()
-    return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
-            "d2h_bytes_per_step": d2h / e2e_steps,
-            "what": "Simulation(model from pinned host arrays) + step() in chunks of "
-                    f"{OUTPUT_FREQ} with observe() after each + final get('pos')"}
-
-
-
-def run_ours(args):
-    import numpy as np
-    import torch
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -359,13 +344,100 @@ def run_ours(args):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def dist_close(dist):
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def time_reps(sim, K: int, min_ms: float, dist=None, max_reps: int = 2000):
+    """fn_step(K) from one saved state, timed with CUDA events on the
+    context's stream and repeated (the state restored between repetitions,
+    outside the events) until min_ms of device time; every rank runs the
+    same number of repetitions.  Returns the per-repetition times (ms); the
+    state is left as it was before."""
+    from fibrenet_b200.ranks import slowest
+    sim.save_state()
+    first = sim.step_timed(K)
+    reps = int(min(max_reps, max(3, math.ceil(min_ms / max(first, 1e-3)))))
+    reps = int(slowest(reps, dist, "cuda"))
+    times = []
+    for _ in range(reps):
+        sim.restore_state()
+        times.append(sim.step_timed(K))
+    sim.restore_state()
+    return times
+
+
+def run_e2e(args, m, local, dist, world, nb, barrier, block=0):
+    """Same metric through the public API with host buffers: model upload from
+    pinned host arrays, RunSimulationLoop in output_freq chunks with the
+    recorded observables read back after each chunk, final state download."""
+    import torch
 
     from fibrenet_b200.native import Simulation
 
-    m = workload(args)
+    e2e_steps = args.steps
+    mm = m.normalised()
+    names = ["pos", "img", "vel", "vel_old", "force", "radius", "mass", "type", "tag", "loc_id",
+             "s_type", "s_p1", "s_p2", "s_rest", "s_k", "s_c1", "s_c2", "a_type", "a_b1", "a_b2",
+             "a_b3", "a_s1", "a_s2", "a_theta0", "a_k"]
+    keep = []
+    for name in names:
+        t = torch.from_numpy(getattr(mm, name)).pin_memory()
+        keep.append(t)
+        setattr(mm, name, t.numpy())
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    w0 = time.perf_counter()
+    sim2 = Simulation(mm, device=local, list_capacity=64, cell_capacity=64, reorder=True,
+                      block_size=block)
+    w1 = time.perf_counter()
+    done = 0
+    obs_bytes = 0
+    while done < e2e_steps:
+        k = min(OUTPUT_FREQ, e2e_steps - done)
+        sim2.step(k)
+        sim2.observe(0, reaction_type=2 if m.n_types > 2 else -1)
+        obs_bytes += 5 * 8
+        done += k
+    w2 = time.perf_counter()
+    final = sim2.get("pos")
+    sim2.sync()
+    e1.record()
+    torch.cuda.synchronize()
+    w3 = time.perf_counter()
+    e2e_ms = max(e0.elapsed_time(e1), 1e3 * (w3 - w0))
+    from fibrenet_b200.ranks import slowest
+    e2e_ms = slowest(e2e_ms, dist, "cuda")
+    h2d = sum(getattr(mm, k).nbytes for k in names)
+    d2h = obs_bytes + final.nbytes
+    e2e_value = world * nb * e2e_steps / (e2e_ms / 1e3)
+    sim2.close()
+    return {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+            "d2h_bytes_per_step": d2h / e2e_steps,
+            "what": "Simulation(model from pinned host arrays) + step() in chunks of "
+                    f"{OUTPUT_FREQ} with observe() after each + final get('pos')",
+            "split_ms": {"upload": 1e3 * (w1 - w0), "steps_and_observe": 1e3 * (w2 - w1),
+                         "download": 1e3 * (w3 - w2)}}
+
+
+def headline(args, m, world, rank, local, dist, e2e=True, cpu=True, label=None):
+    """One network's bead-steps/s line (tensile or dense): autotuned block
+    size, repeated timed region, kernel split, end-to-end leg, CPU baseline."""
+    import torch
+
+    from fibrenet_b200.native import Simulation
+    from fibrenet_b200.ranks import job_rate, slowest
+
+    K = args.steps
     sim = Simulation(m, device=local, list_capacity=64, cell_capacity=64, reorder=True)
     nb = m.n_beads
-
     sim.step(max(args.warmup, 3))
     block = sim.autotune(16)  # block size of the step kernel; the state is restored
     sim.step(8)
@@ -379,136 +451,85 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- timed region: device-resident state, K steps in one RunSimulationLoop call
+    # ---- timed region: device-resident state, fn_step(K) repeated from one state
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
-    sim.enable_timing(True)
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    t0.record()
-    sim.step(args.steps)
-    sim.sync()
-    t1.record()
-    torch.cuda.synchronize()
-    elapsed_ms = t0.elapsed_time(t1)
+    times = time_reps(sim, K, args.min_ms, dist)
     clk = clocks.stop()
+    barrier()
+    med = statistics.median(times)
+    value = job_rate(nb * K, med, dist, "cuda")
+    med = slowest(med, dist, "cuda")
+    # kernel split over one repetition (events around every launch)
+    sim.restore_state()
+    sim.enable_timing(True)
+    sim.step(K)
     kt = sim.kernel_time()
     sim.enable_timing(False)
-    barrier()
-    from fibrenet_b200.ranks import job_rate, slowest
-    value = job_rate(nb * args.steps, elapsed_ms, dist, "cuda")
-    elapsed_ms = slowest(elapsed_ms, dist, "cuda")
+    sim.restore_state()
     stats = sim.stats()
-    launches = 1 + args.steps + kt["rebuilds"] * 7
+    freq = m.settings.grid_update_freq
+    rb = rebuilds_per_call(K, freq)
+    launches_per_call = 1 + K + rb * REBUILD_KERNELS
 
-    # ---- end to end through the public API: model upload from pinned host
-    # buffers, RunSimulationLoop in output_freq chunks with the recorded
-    # observables read back after each chunk, final state download
-    e2e = None
-    if not args.no_e2e:
-        # three end-to-end runs, the median reported: host-side allocation
-        # and page-mapping times on these shared machines vary from run to
-        # run by up to a few hundred ms
-        runs = [run_e2e(args, m, local, dist, world, nb, barrier, block) for _ in range(3)]
-        vals = sorted(r["value"] for r in runs)
-        e2e = dict(runs[0])
-        e2e["value"] = vals[1]
-        e2e["runs"] = [r["value"] for r in runs]
-        e2e["what"] = runs[0]["what"] + " (median of 3 runs)"
-
+    out = {"value": value, "ms_per_step": med / K, "steps": K, "reps": len(times),
+           "timed_steps_total": K * len(times), "rep_ms": {"median": statistics.median(times),
+                                                            "min": min(times), "max": max(times)},
+           "rebuilds_per_step": rb / K, "block": block, "half_pairs": half_pairs, "stats": stats,
+           "kt": kt, "clocks": clk, "gpu_launches": launches_per_call * len(times),
+           "launches_per_call": launches_per_call}
     peak, peak_kind = peaks()
     alg = algorithmic_bytes(m, half_pairs)
     step_ms = kt["step_ms"]
     achieved = alg / (step_ms / 1e3) / 1e9 if step_ms > 0 else None
-    traffic_per_bead = traffic_from_profiles()
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, done_cpu, threads, kind = cpu_reference_rate(m, args.cpu_seconds)
-        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": f"{done_cpu} whole steps of the same {nb}-bead network on the host "
-                         f"(reference kernels as C, OpenMP{''.join(', ' + v for v in ref_note(args).values())})"}
-
-    if rank == 0:
-        line = {
-            "metric": metric_for(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded generator; reference ships no models)",
-            "config": config_dict(m, args, {"half_list_pairs": half_pairs, "block_size": block,
-                                            "storage": "positions f64, velocities/forces f32"}),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None,
-                         "peak_kind": peak_kind,
-                         "kernel": "k_step (force + kick + drift, one launch per step)",
-                         "algorithmic_bytes_per_launch": alg,
-                         "layout_bytes_per_launch": layout_bytes(m, half_pairs, stats["bond_path"] == 2),
-                         "step_kernel_ms": step_ms, "rebuild_ms": kt["rebuild_ms"],
-                         "traffic": (traffic_per_bead * nb) if traffic_per_bead else None},
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": int(launches),
-            "clocks": clk,
-            "overflow": {"cell": stats["cell_overflow"], "list": stats["list_overflow"]},
-        }
-        print(json.dumps(line), flush=True)
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                       "kernel": "step kernel (force + kick + drift, one launch per step)",
+                       "algorithmic_bytes_per_launch": alg,
+                       "layout_bytes_per_launch": layout_bytes(m, half_pairs, stats["bond_path"] == 2),
+                       "step_kernel_ms": step_ms, "rebuild_ms": kt["rebuild_ms"],
+                       "whole_step_frac": alg / (med / K / 1e3) / 1e9 / peak}
     sim.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+
+    if e2e and not args.no_e2e:
+        # three end-to-end runs, the median reported: host-side allocation
+        # and page-mapping times on these shared machines vary from run to run
+        runs = [run_e2e(args, m, local, dist, world, nb, barrier, block) for _ in range(3)]
+        order = sorted(range(3), key=lambda i: runs[i]["value"])
+        e2e_line = dict(runs[order[1]])
+        e2e_line["runs"] = [r["value"] for r in runs]
+        e2e_line["what"] = runs[0]["what"] + " (median of 3 runs)"
+        out["e2e"] = e2e_line
+    if cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, done_cpu, threads, kind = cpu_reference_rate(m, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                               "sample": f"{done_cpu} whole steps of the same {nb}-bead network on "
+                                         f"the host in calls of 8 (reference kernels as C, OpenMP"
+                                         f"{''.join(', ' + v for v in ref_note(args).values())})"}
+    return out
 
 
-def run_ensemble(args):
+def ensemble_result(args, local, dist, world, rank, steps: int = 100, networks: int = 256):
     """Batched ensemble: the networks in one context (one launch per kernel
     for all of them, steps replayed as CUDA graphs, tuned block size) against
     the same networks each in its own context, run one after the other."""
-    import torch
-
     from fibrenet_b200 import generate as g
     from fibrenet_b200.native import Simulation
     from fibrenet_b200.ranks import job_rate, partition_networks, slowest
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA device")
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    all_ms = g.ensemble_networks(seed=3, n_networks=args.networks)
-    # independent networks: split by bead count, no exchange between ranks
+    all_ms = g.ensemble_networks(seed=3, n_networks=networks)
     mine = partition_networks([m.n_beads for m in all_ms], world)[rank]
     ms = [all_ms[i] for i in mine]
     nb = sum(m.n_beads for m in ms)
     nb_all = sum(m.n_beads for m in all_ms)
-    K = args.steps
-
-    def timed(sim, steps):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        sim.sync()
-        torch.cuda.synchronize()
-        e0.record()
-        sim.step(steps)
-        sim.sync()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
-
+    K = steps
     batched = Simulation(ms, device=local, list_capacity=32, reorder=True, use_graphs=True)
     batched.step(max(args.warmup, 3))
     block = batched.autotune(16)
     batched.step(8)
-    clocks = ClockSampler(0)
-    clocks.start()
-    t_batched = timed(batched, K)
-    clk = clocks.stop()
+    batched.sync()
+    clocks = ClockSampler(local).start()
+    t_batched = statistics.median(time_reps(batched, K, 300.0, dist, max_reps=20))
     batched.enable_timing(True)
     batched.step(16)
     kt = batched.kernel_time()
@@ -517,33 +538,26 @@ def run_ensemble(args):
     for m in ms:
         one = Simulation(m, device=local, list_capacity=32, reorder=True, use_graphs=True)
         one.step(max(args.warmup, 3))
-        t_single += timed(one, K)
+        one.sync()
+        one.step_timed(K)  # graphs of this call length captured
+        t_single += one.step_timed(K)
         one.close()
-    if dist is not None:
-        dist.barrier()
+    clk = clocks.stop()
     v_b = job_rate(nb * K, t_batched, dist, "cuda")
     v_s = job_rate(nb * K, t_single, dist, "cuda")
     t_batched = slowest(t_batched, dist, "cuda")
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    line = {"metric": "bead-steps/s (256-network ensemble, batched in one launch per kernel)",
-            "value": v_b, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(args.warmup, 3),
-            "ms_per_step": t_batched / K, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": f"ensemble_{len(all_ms)}", "networks": len(all_ms), "beads": nb_all,
-                       "parallelism": f"networks split over {world} rank(s) by bead count",
-                       "fibres_per_network": "U[50, 2000] x 50 beads", "block_size": block,
-                       "graphs": True},
-            "one_by_one": {"value": v_s, "ms_per_step_all_networks": t_single / K},
-            "batched_over_one_by_one": v_b / v_s,
-            "step_kernel_ms": kt["step_ms"], "rebuild_ms": kt["rebuild_ms"], "clocks": clk}
-    print(json.dumps(line), flush=True)
+    return {"workload": f"ensemble_{len(all_ms)}", "networks": len(all_ms), "beads": nb_all,
+            "steps": K, "fibres_per_network": "U[50, 2000] x 50 beads", "graphs": True,
+            "block_size": block, "batched_bead_steps_per_s": v_b, "one_by_one_bead_steps_per_s": v_s,
+            "batched_over_one_by_one": v_b / v_s, "batched_ms_per_step": t_batched / K,
+            "one_by_one_ms_per_step": t_single / K, "step_kernel_ms": kt["step_ms"],
+            "rebuild_ms": kt["rebuild_ms"], "clocks": clk,
+            "timing": "fn_step(K) with CUDA events on the context stream; batched: median of "
+                      "repetitions from one state; one by one: sum over the networks of one "
+                      "timed call each after a call of the same length"}
 
 
-def run_adjoint(args):
+def adjoint_result(args, local, dist, world, rank, networks: int = 64, steps: int = 2000):
     """Stiffness fitting: 64 tensile networks in one context, loss = squared
     error of the x reaction curve (sampled every 20 steps) against a target
     run with lognormal(0, 0.2)-perturbed stiffnesses.  Times the plain
@@ -554,23 +568,11 @@ def run_adjoint(args):
 
     from fibrenet_b200 import generate as g
     from fibrenet_b200.fitting import ReactionCurve
-    from fibrenet_b200.ranks import partition_networks
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA device")
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from fibrenet_b200.ranks import partition_networks, slowest, total
     every, ckpt = 20, 100
-    steps = max(ckpt, (args.steps // ckpt) * ckpt)
+    steps = max(ckpt, (steps // ckpt) * ckpt)
     nsamples = steps // every
-    all_ms = g.fitting_networks(seed=4, n_networks=args.networks)
+    all_ms = g.fitting_networks(seed=4, n_networks=networks)
     mine = partition_networks([m.n_beads for m in all_ms], world)[rank]
     ms = [all_ms[i] for i in mine]
     nb = sum(m.n_beads for m in ms)
@@ -598,6 +600,7 @@ def run_adjoint(args):
     # warm-up: graphs, replay buffers
     R = curve.run(k0, r0, a0)
     curve.sim.adjoint_backward(np.zeros_like(R))
+    obs = torch.zeros(5, dtype=torch.float64, device=f"cuda:{local}")
 
     def plain():
         curve._load(k0, r0, a0, None)
@@ -613,9 +616,7 @@ def run_adjoint(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    obs = torch.zeros(5, dtype=torch.float64, device=f"cuda:{local}")
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks = ClockSampler(local).start()
     t_plain = plain()
     curve._load(k0, r0, a0, None)
     R, t_fwd = timed(lambda: curve.sim.adjoint_forward(nsamples, every, ckpt, CR))
@@ -644,7 +645,6 @@ def run_adjoint(args):
                "median_rel_err_k_start": float(np.median(np.abs(k0 / true_k - 1))),
                "median_rel_err_k_fit": float(np.median(np.abs(k_fit / true_k - 1)))}
     curve.close()
-    from fibrenet_b200.ranks import slowest, total
     # networks are independent: the loss and the bead count add up over the
     # ranks, times are the slowest rank's, gradient norms combine as squares
     t_plain, t_fwd, t_bwd = (slowest(t, dist, "cuda") for t in (t_plain, t_fwd, t_bwd))
@@ -655,101 +655,129 @@ def run_adjoint(args):
     if fit is not None:
         fit["loss_first"] = total(fit["loss_first"], dist, "cuda")
         fit["loss_last"] = total(fit["loss_last"], dist, "cuda")
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    line = {"metric": "adjoint/forward time (64-network tensile fit)",
-            "value": t_bwd / t_plain, "unit": "ratio", "n_gpus": world, "steps": steps, "warmup": 1,
-            "ms_per_step": t_bwd / steps, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 forces / f32 state / f64 gradient sums",
-            "data": "synthetic (seeded generator; target from lognormal(0, 0.2) stiffness factors)",
-            "config": {"workload": f"fit_{len(all_ms)}", "networks": len(all_ms), "beads": nb_all,
-                       "every": every, "checkpoint_every": ckpt, "loss": "sum (R_x - R*_x)^2",
-                       "params": {"spring_k": len(k0), "spring_rest": len(r0), "angle_k": len(a0),
-                                  "pos0": 3 * nb, "per": "rank 0"},
-                       "parallelism": f"networks split over {world} rank(s) by bead count"},
-            "forward_ms": t_plain, "recorded_forward_ms": t_fwd, "backward_ms": t_bwd,
+    return {"workload": f"fit_{len(all_ms)}", "networks": len(all_ms), "beads": nb_all,
+            "steps": steps, "every": every, "checkpoint_every": ckpt,
+            "adjoint_over_forward": t_bwd / t_plain, "forward_ms": t_plain,
+            "recorded_forward_ms": t_fwd, "backward_ms": t_bwd,
             "forward_bead_steps_per_s": nb_all * steps / (t_plain / 1e3),
-            "backward_over_recorded_forward": t_bwd / t_fwd, "loss": loss0,
-            "grad_norm": gnorm,
-            "fit": fit, "clocks": clk}
-    print(json.dumps(line), flush=True)
+            "backward_over_recorded_forward": t_bwd / t_fwd, "loss": loss0, "grad_norm": gnorm,
+            "loss_def": "sum (R_x - R*_x)^2", "fit": fit, "clocks": clk,
+            "params": {"spring_k": len(k0), "spring_rest": len(r0), "angle_k": len(a0)}}
 
 
-def run_plain(args):
+def plain_result(args, local, dist, steps: int = 2000):
     """The small network (200 fibres x 50 beads, penalty contacts): its working
     set sits in L2, so the step is launch- and latency-bound; steps run as
-    CUDA graphs, timed with CUDA events, then the kernels alone with timing."""
-    import torch
-
+    CUDA graphs, timed with CUDA events on the context stream."""
     from fibrenet_b200 import generate as g
     from fibrenet_b200.native import Simulation
     from fibrenet_b200.ranks import job_rate, slowest
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA device")
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     m = g.plain_network(seed=0)
     sim = Simulation(m, device=local, list_capacity=64, reorder=True, use_graphs=True)
     sim.step(max(args.warmup, 3))
     block = sim.autotune(64)  # 10k beads fill few SMs at the default block size
     sim.step(8)
     sim.sync()
-    K = args.steps
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    clocks = ClockSampler(local)
-    clocks.start()
-    torch.cuda.synchronize()
-    e0.record()
-    sim.step(K)
-    sim.sync()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    clocks = ClockSampler(local).start()
+    times = time_reps(sim, steps, 300.0, dist, max_reps=10)
     clk = clocks.stop()
+    med = statistics.median(times)
     sim.enable_timing(True)
-    sim.step(min(K, 400))
+    sim.step(min(steps, 400))
     kt = sim.kernel_time()
     sim.close()
-    value = job_rate(m.n_beads * K, ms, dist, "cuda")
-    ms = slowest(ms, dist, "cuda")
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    line = {"metric": "bead-steps/s (10k-bead network, steps as CUDA graphs)", "value": value,
-            "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(args.warmup, 3),
-            "ms_per_step": ms / K, "us_per_step": 1e3 * ms / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": config_dict(m, args, {"graphs": True, "block_size": block,
-                                            "l2": "working set in L2 (launch- and "
-                                            "latency-bound, not measured against HBM)"}),
-            "step_kernel_us": 1e3 * kt["step_ms"], "rebuild_us": 1e3 * kt["rebuild_ms"], "clocks": clk}
-    print(json.dumps(line), flush=True)
+    value = job_rate(m.n_beads * steps, med, dist, "cuda")
+    med = slowest(med, dist, "cuda")
+    return {"workload": "plain_10k", "beads": m.n_beads, "steps": steps, "value": value,
+            "us_per_step": 1e3 * med / steps, "graphs": True, "block_size": block,
+            "step_kernel_us": 1e3 * kt["step_ms"], "rebuild_us": 1e3 * kt["rebuild_ms"],
+            "clocks": clk, "l2": "working set in L2 (launch- and latency-bound)"}
+
+
+def dense_result(args, local, dist, world, rank):
+    m = dense_model(40000)
+    r = headline(args, m, world, rank, local, dist, e2e=False, cpu=False)
+    return {"workload": "dense_4M", "beads": m.n_beads, "value": r["value"],
+            "ms_per_step": r["ms_per_step"], "steps": r["steps"], "reps": r["reps"],
+            "block_size": r["block"], "step_kernel_ms": r["kt"]["step_ms"],
+            "rebuild_ms": r["kt"]["rebuild_ms"], "roofline_frac": r["roofline"]["frac"],
+            "half_list_pairs": r["half_pairs"], "clocks": r["clocks"],
+            "overflow": {"cell": r["stats"]["cell_overflow"], "list": r["stats"]["list_overflow"]}}
+
+
+def run_ours(args):
+    world, rank, local, dist = dist_setup()
+    m = workload(args)
+    r = headline(args, m, world, rank, local, dist)
+    extras = {}
+    if world == 1 and not args.no_extras and args.workload == "tensile":
+        extras["ensemble"] = ensemble_result(args, local, dist, world, rank)
+        extras["adjoint"] = adjoint_result(args, local, dist, world, rank)
+        extras["dense"] = dense_result(args, local, dist, world, rank)
+        extras["plain"] = plain_result(args, local, dist)
+    if rank == 0:
+        line = {
+            "metric": metric_for(args), "value": r["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator; reference ships no models)",
+            "config": config_dict(m, args, {"half_list_pairs": r["half_pairs"], "block_size": r["block"],
+                                            "storage": "positions f64, velocities/forces f32",
+                                            "timed_region": f"fn_step({args.steps}) from one saved state, "
+                                                            f"{r['reps']} repetitions, median"}),
+            "reps": r["reps"], "timed_steps_total": r["timed_steps_total"], "rep_ms": r["rep_ms"],
+            "rebuilds_per_step": r["rebuilds_per_step"],
+            "roofline": r["roofline"], "cpu_baseline": r.get("cpu_baseline"), "e2e": r.get("e2e"),
+            "gpu_launches": r["gpu_launches"], "launches_per_call": r["launches_per_call"],
+            "clocks": r["clocks"],
+            "overflow": {"cell": r["stats"]["cell_overflow"], "list": r["stats"]["list_overflow"]},
+        }
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    dist_close(dist)
+
+
+def run_single_workload(args):
+    """--workload ensemble | adjoint | plain: that sub-result alone as the line."""
+    world, rank, local, dist = dist_setup()
+    if args.workload == "ensemble":
+        r = ensemble_result(args, local, dist, world, rank, steps=args.steps, networks=args.networks)
+        line = {"metric": "bead-steps/s (256-network ensemble, batched in one launch per kernel)",
+                "value": r["batched_bead_steps_per_s"], "unit": UNIT, "n_gpus": world, "steps": r["steps"],
+                "warmup": max(args.warmup, 3), "ms_per_step": r["batched_ms_per_step"],
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator)",
+                "config": {"workload": r["workload"], "networks": r["networks"], "beads": r["beads"],
+                           "parallelism": f"networks split over {world} rank(s) by bead count"}}
+    elif args.workload == "adjoint":
+        r = adjoint_result(args, local, dist, world, rank, networks=args.networks, steps=max(args.steps, 100))
+        line = {"metric": "adjoint/forward time (64-network tensile fit)",
+                "value": r["adjoint_over_forward"], "unit": "ratio", "n_gpus": world, "steps": r["steps"],
+                "warmup": 1, "ms_per_step": r["backward_ms"] / r["steps"], "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64 forces / f32 state / f64 gradient sums",
+                "data": "synthetic (seeded generator; target from lognormal(0, 0.2) stiffness factors)",
+                "config": {"workload": r["workload"], "networks": r["networks"], "beads": r["beads"],
+                           "parallelism": f"networks split over {world} rank(s) by bead count"}}
+    else:
+        r = plain_result(args, local, dist, steps=args.steps)
+        line = {"metric": "bead-steps/s (10k-bead network, steps as CUDA graphs)", "value": r["value"],
+                "unit": UNIT, "n_gpus": world, "steps": r["steps"], "warmup": max(args.warmup, 3),
+                "ms_per_step": r["us_per_step"] / 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+                "config": {"workload": "plain_10k", "beads": r["beads"]}}
+    line["result"] = r
+    dist_close(dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
-    elif args.workload == "ensemble":
-        run_ensemble(args)
-    elif args.workload == "adjoint":
-        run_adjoint(args)
-    elif args.workload == "plain":
-        run_plain(args)
+    elif args.workload in ("ensemble", "adjoint", "plain"):
+        run_single_workload(args)
     else:
         run_ours(args)
 

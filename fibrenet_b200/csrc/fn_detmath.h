@@ -11,9 +11,11 @@
  *   acos(x) = 2 asin(sqrt((1-x)/2)),     x  >  1/2
  *   acos(x) = pi - 2 asin(sqrt((1+x)/2)), x < -1/2
  * R(z) = (asin(sqrt z) - sqrt z) / z^1.5 on [0, 1/4] is replaced by its
- * degree-13 Chebyshev interpolant (fitted at 60 digits with mpmath, written
- * in monomial form); the interpolation error is below 3e-19 relative to
- * asin, so the result is within a few ulp of acos.
+ * degree-13 interpolant at the Chebyshev points of the first kind (60-digit
+ * arithmetic with mpmath, written in monomial form and rounded to doubles;
+ * tests/detmath_fit.py regenerates the coefficients); the interpolation
+ * error is below 3e-19 relative to asin, so the result is within a few ulp
+ * of acos.
  */
 #ifndef FIBRENET_DETMATH_H
 #define FIBRENET_DETMATH_H

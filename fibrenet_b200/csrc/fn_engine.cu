@@ -212,6 +212,7 @@ void free_all(fn_ctx* c) {
     dfree(c, c->en_partial);
     dfree(c, c->en_out);
     dfree(c, c->series);
+    dfree(c, c->snap);
     adjoint_free(c);
 }
 
@@ -980,6 +981,7 @@ static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) 
     CK(cudaStreamSynchronize(c->stream));
     drop_graphs(c);
     c->uploaded = false;
+    c->snap_valid = false;
     c->n_nets = n_networks;
     c->nets_h.assign(n_networks, FnNet{});
     c->info.assign(n_networks, NetHost{});
@@ -1643,8 +1645,19 @@ FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_s
 
 namespace {
 
-/* Observables of network `net` into out[0..4] on the context's stream. */
-int observe_async(fn_ctx* c, int net, int reaction_type, double* out) {
+/* Blocks of 256 threads of the observables reduction of network `net`: one
+   per 256 beads, springs or angles, at most 1024 (each block then loops), so
+   the partial sums and their order depend on the network alone. */
+int observe_blocks(const fn_ctx* c, int net) {
+    const NetHost& h = c->info[net];
+    const long long span = std::max({(long long)(h.bead_end - h.bead_begin), (long long)(h.spring_end - h.spring_begin),
+                                     (long long)(h.angle_end - h.angle_begin), 1LL});
+    return (int)std::min<long long>(1024, (span + 255) / 256);
+}
+
+/* Observables of network `net` into out[0..4] on the context's stream, with
+   the partial sums in `partial` (5 doubles per block). */
+int observe_into(fn_ctx* c, int net, int reaction_type, double* partial, double* out) {
     const NetHost& h = c->info[net];
     fn::ObserveArgs O{};
     O.ch_flags = c->chain ? c->ch_flags.p : nullptr;
@@ -1660,12 +1673,13 @@ int observe_async(fn_ctx* c, int net, int reaction_type, double* out) {
     O.angle_begin = h.angle_begin;
     O.angle_end = h.angle_end;
     O.reaction_type = reaction_type;
-    O.partial = c->obs_partial.p;
-    long long span = std::max({(long long)(h.bead_end - h.bead_begin), (long long)(h.spring_end - h.spring_begin),
-                               (long long)(h.angle_end - h.angle_begin), 1LL});
-    int nblocks = (int)std::min<long long>(1024, (span + 255) / 256);
-    CK(fn::launch_observe(O, nblocks, out, c->stream));
+    O.partial = partial;
+    CK(fn::launch_observe(O, observe_blocks(c, net), out, c->stream));
     return FN_OK;
+}
+
+int observe_async(fn_ctx* c, int net, int reaction_type, double* out) {
+    return observe_into(c, net, reaction_type, c->obs_partial.p, out);
 }
 
 /* Energy and virial of network `net` into out[0..FN_EN_N) on the stream. */
@@ -1998,6 +2012,111 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     FN_CATCH(c)
 }
 
+/* The dynamic state a step changes, as (device pointer, bytes) pairs in a
+   fixed order: positions and images of the current ping-pong half,
+   velocity_old, force, velocity, spring/angle statuses (both layouts), the
+   device counters and, in displacement mode, the reference images and the
+   rebuild gate.  Contact lists are not state: every fn_step call rebuilds
+   them at its step 0. */
+static std::vector<std::pair<void*, size_t>> state_arrays(fn_ctx* c) {
+    const size_t nb = (size_t)c->nb;
+    std::vector<std::pair<void*, size_t>> v;
+    v.emplace_back(c->pos[c->cur].p, sizeof(double4) * nb);
+    v.emplace_back(c->img[c->cur].p, sizeof(double4) * nb);
+    v.emplace_back(c->vold.p, sizeof(float4) * nb);
+    v.emplace_back(c->force.p, sizeof(float4) * nb);
+    v.emplace_back(c->vel.p, sizeof(float4) * nb);
+    v.emplace_back(c->sp_status.p, (size_t)c->ns);
+    v.emplace_back(c->an_status.p, (size_t)c->na);
+    if (c->chain) v.emplace_back(c->ch_status.p, nb);
+    v.emplace_back(c->counters.p, sizeof(unsigned long long) * FN_CNT_N);
+    if (c->verlet) {
+        v.emplace_back(c->ref_img.p, sizeof(double4) * nb);
+        v.emplace_back(c->gate.p, sizeof(int));
+    }
+    return v;
+}
+
+/* Device-side snapshot of the dynamic state (no counterpart in the reference,
+   whose restart files go through the host): one device buffer held by the
+   context, copied on its stream. */
+FN_API int fn_state_save(fn_ctx* c) {
+    FN_TRY
+    int r = check_ready(c);
+    if (r) return r;
+    CK(cudaSetDevice(c->cfg.device));
+    const auto arrs = state_arrays(c);
+    size_t total = 0;
+    for (const auto& a : arrs) total += (a.second + 255) / 256 * 256;
+    if (c->snap.n < total) CK(dalloc(c, c->snap, total));
+    size_t off = 0;
+    for (const auto& a : arrs) {
+        if (a.first && a.second)
+            CK(cudaMemcpyAsync(c->snap.p + off, a.first, a.second, cudaMemcpyDeviceToDevice, c->stream));
+        off += (a.second + 255) / 256 * 256;
+    }
+    c->snap_valid = true;
+    c->snap_cur = c->cur;
+    c->snap_steps = c->steps_done;
+    c->snap_rebuilds = c->rebuilds_done;
+    return FN_OK;
+    FN_CATCH(c)
+}
+
+FN_API int fn_state_restore(fn_ctx* c) {
+    FN_TRY
+    if (c) c->state_version++;
+    int r = check_ready(c);
+    if (r) return r;
+    if (!c->snap_valid) return fail(c, FN_ERR_STATE, "fn_state_restore: no snapshot (call fn_state_save first)");
+    CK(cudaSetDevice(c->cfg.device));
+    c->cur = c->snap_cur;
+    const auto arrs = state_arrays(c);
+    size_t off = 0;
+    for (const auto& a : arrs) {
+        if (a.first && a.second)
+            CK(cudaMemcpyAsync(a.first, c->snap.p + off, a.second, cudaMemcpyDeviceToDevice, c->stream));
+        off += (a.second + 255) / 256 * 256;
+    }
+    c->steps_done = c->snap_steps;
+    c->rebuilds_done = c->snap_rebuilds;
+    return FN_OK;
+    FN_CATCH(c)
+}
+
+/* fn_step bracketed by CUDA events on the context's stream; waits for the
+   second event and returns the device time between them. */
+FN_API int fn_step_timed(fn_ctx* c, int nsteps, double* ms) {
+    FN_TRY
+    int r = check_ready(c);
+    if (r) return r;
+    if (!ms) return fail(c, FN_ERR_ARG, "fn_step_timed: null output");
+    CK(cudaSetDevice(c->cfg.device));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(c, FN_ERR_CUDA, "fn_step_timed: cudaEventCreate");
+    }
+    cudaError_t e = cudaEventRecord(e0, c->stream);
+    if (e == cudaSuccess) {
+        r = fn_step(c, nsteps);
+        if (r == FN_OK) {
+            e = cudaEventRecord(e1, c->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float f = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+            *ms = f;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (r) return r;
+    if (e != cudaSuccess) return fail(c, FN_ERR_CUDA, std::string("fn_step_timed: ") + cudaGetErrorString(e));
+    return FN_OK;
+    FN_CATCH(c)
+}
+
 /* Forces alone at the current positions (zeroed, no base term), for the
    one-step parity checks: terms bit 0 springs, 1 angles, 2 contacts. */
 FN_API int fn_forces_only(fn_ctx* c, int terms) {
@@ -2020,11 +2139,13 @@ FN_API int fn_forces_only(fn_ctx* c, int terms) {
 /* ======================================================================== */
 /* Observables without any device allocation.                               */
 
-/* Partial sums of the observables reduction: one slot of 5 doubles per block
-   of 256 items, for at most FN_OBSERVE_NOALLOC_MAX_BLOCKS blocks.  It lives in
-   the library image, so every GPU that loads the library holds these 320 KB
-   until the process exits, and every call shares them. */
-#define FN_OBSERVE_NOALLOC_MAX_BLOCKS 8192
+/* Partial sums of the observables reduction: one slot of 5 doubles per block,
+   for the FN_OBSERVE_NOALLOC_MAX_BLOCKS blocks that fn_observe's reduction
+   uses at most (larger networks loop inside each block), so any network fits
+   and the sums are fn_observe's, bit for bit.  It lives in the library image:
+   every GPU that loads the library holds these 40 KB until the process exits,
+   and every call shares them. */
+#define FN_OBSERVE_NOALLOC_MAX_BLOCKS 1024
 static __device__ __align__(256) double fn_observe_scratch[5 * FN_OBSERVE_NOALLOC_MAX_BLOCKS];
 
 namespace {
@@ -2032,7 +2153,10 @@ namespace {
 /* Device address of fn_observe_scratch on each device, looked up once per
    device.  In host code the array's name only stands in for the symbol; its
    address on a device comes from cudaGetSymbolAddress with that device
-   current. */
+   current.  The cached address belongs to the device's primary context: a
+   cudaDeviceReset (or any other teardown of that context) makes it stale, so
+   a process that resets a device must not call fn_observe_noalloc on it
+   afterwards. */
 constexpr int FN_NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_scratch[FN_NOALLOC_MAX_DEVICES] = {};
@@ -2058,41 +2182,21 @@ int noalloc_scratch(fn_ctx* c, double** out) {
 
 extern "C" FN_API int fn_observe_noalloc(fn_ctx* c, int net, int reaction_type, double* out_device) {
     FN_TRY
+    fnh::NvtxRange nvtx_range_("fn_observe_noalloc");
     int r = check_ready(c);
     if (r) return r;
     if (!out_device || net < 0 || net >= c->n_nets)
         return fail(c, FN_ERR_ARG, "fn_observe_noalloc: bad arguments");
-    const NetHost& h = c->info[net];
-    const long long span = std::max({(long long)(h.bead_end - h.bead_begin),
-                                     (long long)(h.spring_end - h.spring_begin),
-                                     (long long)(h.angle_end - h.angle_begin), 1LL});
-    const long long nblocks = (span + 255) / 256;
-    if (nblocks > FN_OBSERVE_NOALLOC_MAX_BLOCKS)
+    const int nblocks = observe_blocks(c, net);
+    if (nblocks > FN_OBSERVE_NOALLOC_MAX_BLOCKS) /* guards the scratch should the block rule change */
         return fail(c, FN_ERR_CAPACITY,
-                    "fn_observe_noalloc: network " + std::to_string(net) + " has " +
-                        std::to_string(span) + " beads/springs/angles; the static scratch holds " +
-                        std::to_string((long long)FN_OBSERVE_NOALLOC_MAX_BLOCKS * 256) +
-                        " at most (use fn_observe)");
+                    "fn_observe_noalloc: the reduction needs " + std::to_string(nblocks) +
+                        " partial sums; the static scratch holds " +
+                        std::to_string(FN_OBSERVE_NOALLOC_MAX_BLOCKS) + " (use fn_observe)");
     CK(cudaSetDevice(c->cfg.device));
     double* scratch = nullptr;
     r = noalloc_scratch(c, &scratch);
     if (r) return r;
-    fn::ObserveArgs O{};
-    O.ch_flags = c->chain ? c->ch_flags.p : nullptr;
-    O.ch_status = c->chain ? c->ch_status.p : nullptr;
-    O.pos = c->pos[c->cur].p;
-    O.force = c->force.p;
-    O.sp_status = c->sp_status.p;
-    O.an_status = c->an_status.p;
-    O.bead_begin = h.bead_begin;
-    O.bead_end = h.bead_end;
-    O.spring_begin = h.spring_begin;
-    O.spring_end = h.spring_end;
-    O.angle_begin = h.angle_begin;
-    O.angle_end = h.angle_end;
-    O.reaction_type = reaction_type;
-    O.partial = scratch;
-    CK(fn::launch_observe(O, (int)nblocks, out_device, c->stream));
-    return FN_OK;
+    return observe_into(c, net, reaction_type, scratch, out_device);
     FN_CATCH(c)
 }

@@ -134,6 +134,12 @@ struct fn_ctx {
     DevBuf<double4> ref_img;     /* image positions at the last rebuild */
     DevBuf<int> gate;            /* 1: rebuild before the next step */
 
+    /* device snapshot of the dynamic state (fn_state_save / fn_state_restore) */
+    DevBuf<unsigned char> snap;
+    bool snap_valid = false;
+    int snap_cur = 0;
+    long long snap_steps = 0, snap_rebuilds = 0;
+
     /* bumped by every call that changes the state or the parameters */
     long long state_version = 0;
     /* differentiation state (fn_adjoint_*), null until first used */
@@ -146,7 +152,7 @@ int fail(fn_ctx* c, int code, const std::string& msg);
 
 /* Named NVTX range over a host-side phase (upload, a RunSimulationLoop call,
    a contact rebuild, a download, ...): a profiler groups the kernels launched
-   inside it by that name (ncu --nvtx --nvtx-include "fn_rebuild/"); without a
+   inside it by that name (ncu --clock-control none --nvtx --nvtx-include "fn_rebuild/"); without a
    profiler attached a push/pop costs a few nanoseconds. */
 struct NvtxRange {
     explicit NvtxRange(const char* name) { nvtxRangePushA(name); }

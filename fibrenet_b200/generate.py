@@ -33,7 +33,7 @@ def _directions(rng, n, tilt_deg, mode):
 
 
 def place_fibres(rng, n_fibres, beads, box, periodic, z_range=None, tilt_deg=5.0,
-                 orient="xy", spacing=1.0, min_sep=None, max_tries=200):
+                 orient="xy", spacing=1.0, min_sep=None, max_tries=200, placement="native"):
     """Returns unwrapped bead positions [n_fibres, beads, 3].
 
     Centres are uniform in the box (z in ``z_range`` if given); on finite axes
@@ -41,7 +41,10 @@ def place_fibres(rng, n_fibres, beads, box, periodic, z_range=None, tilt_deg=5.0
     new fibre must keep that distance from every bead already placed (minimum
     image on periodic axes): for a drawn (x, y, direction) the centre height is
     chosen uniformly among the heights that satisfy it, and the draw is
-    repeated when none does.
+    repeated when none does.  ``placement`` picks the implementation of the
+    separated placement: "native" (fn_place_fibres in the library) or "host"
+    (numpy, no native code; a different random stream, so a different but
+    equally distributed network).
     """
     box = np.asarray(box, np.float64)
     off = (np.arange(beads) - (beads - 1) / 2.0) * spacing
@@ -63,6 +66,9 @@ def place_fibres(rng, n_fibres, beads, box, periodic, z_range=None, tilt_deg=5.0
             out[done:done + len(pts)] = pts
             done += len(pts)
         return out
+    if placement == "host":
+        return _place_separated(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg, orient,
+                                off, float(min_sep), max_tries)
     return _place_separated_native(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg,
                                    orient, spacing, float(min_sep), max_tries)
 
@@ -90,15 +96,21 @@ def _place_separated_native(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_
 
 def _place_separated(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg, orient, off, rmin,
                      max_tries):
+    """Separated placement in numpy (no native code; the algorithm of
+    fn_place_fibres): for a drawn (x, y, direction) the z intervals where some
+    placed bead would come closer than rmin are blocked, and the centre height
+    is drawn uniformly from what is left of the admissible range."""
     # columns of size >= rmin in x and y; each keeps the (x, y, z) of its beads
     ncx = max(1, int(box[0] // rmin))
     ncy = max(1, int(box[1] // rmin))
     cw = np.array([box[0] / ncx, box[1] / ncy])
     cap = 32
-    col = np.zeros((ncx, ncy, cap, 3))
-    coln = np.zeros((ncx, ncy), np.int64)
+    col = np.zeros((ncx * ncy, cap, 3))
+    coln = np.zeros(ncx * ncy, np.int64)
     out = np.zeros((n_fibres, beads, 3))
     r2 = rmin * rmin
+    dxy = np.array([(dx, dy) for dx in (-1, 0, 1) for dy in (-1, 0, 1)], np.int64)  # [9, 2]
+    slot = np.arange(cap)
     for f in range(n_fibres):
         for _ in range(max_tries):
             c = rng.uniform(0.0, 1.0, 3) * box
@@ -119,63 +131,58 @@ def _place_separated(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg, or
                 hi = min(hi, box[2] - rel[:, 2].max())
             if hi <= lo:
                 continue
-            # neighbouring columns of every bead
-            ix = np.floor(pts[:, 0] / cw[0]).astype(np.int64)
-            iy = np.floor(pts[:, 1] / cw[1]).astype(np.int64)
-            blocks = []
-            for dx in (-1, 0, 1):
-                for dy in (-1, 0, 1):
-                    jx = ix + dx
-                    jy = iy + dy
-                    okx = (jx >= 0) & (jx < ncx)
-                    oky = (jy >= 0) & (jy < ncy)
-                    if periodic[0]:
-                        jx = jx % ncx
-                        okx[:] = True
-                    if periodic[1]:
-                        jy = jy % ncy
-                        oky[:] = True
-                    sel = np.nonzero(okx & oky)[0]
-                    if len(sel) == 0:
-                        continue
-                    n = coln[jx[sel], jy[sel]]
-                    if n.max(initial=0) == 0:
-                        continue
-                    cand = col[jx[sel], jy[sel]]  # [k, cap, 3]
-                    valid = np.arange(cap)[None, :] < n[:, None]
-                    dxy = cand[:, :, :2] - pts[sel, None, :2]
-                    for a in range(2):
-                        if periodic[a]:
-                            dxy[..., a] -= box[a] * np.round(dxy[..., a] / box[a])
-                    q = (dxy ** 2).sum(-1)
-                    hit = valid & (q < r2)
-                    if hit.any():
-                        kk, ss = np.nonzero(hit)
-                        h = np.sqrt(r2 - q[kk, ss])
-                        zc = cand[kk, ss, 2] - rel[sel[kk], 2]
-                        blocks.append(np.stack([zc - h, zc + h], axis=1))
-            if blocks:
-                iv = np.concatenate(blocks)
-                if periodic[2]:
-                    iv = np.concatenate([iv, iv - box[2], iv + box[2]])
-                iv = iv[np.argsort(iv[:, 0])]
-                free = []
-                cur = lo
-                for a0, a1 in iv:
-                    if a0 > cur:
-                        free.append((cur, min(a0, hi)))
-                    cur = max(cur, a1)
-                    if cur >= hi:
-                        break
-                if cur < hi:
-                    free.append((cur, hi))
-                free = [(a, b) for a, b in free if b > a]
-                if not free:
-                    continue
-                lens = np.array([b - a for a, b in free])
-                k = rng.choice(len(free), p=lens / lens.sum())
-                zc = rng.uniform(*free[k])
+            # the 3 x 3 neighbouring columns of every bead, all at once
+            jx = np.floor(pts[:, 0] / cw[0]).astype(np.int64)[None, :] + dxy[:, 0, None]  # [9, B]
+            jy = np.floor(pts[:, 1] / cw[1]).astype(np.int64)[None, :] + dxy[:, 1, None]
+            ok = np.ones(jx.shape, bool)
+            if periodic[0]:
+                jx %= ncx
             else:
+                ok &= (jx >= 0) & (jx < ncx)
+            if periodic[1]:
+                jy %= ncy
+            else:
+                ok &= (jy >= 0) & (jy < ncy)
+            kk, bb = np.nonzero(ok)
+            cid = jx[kk, bb] * ncy + jy[kk, bb]
+            n = coln[cid]
+            zc = None
+            if n.max(initial=0) > 0:
+                sel = n > 0
+                cid, bb, n = cid[sel], bb[sel], n[sel]
+                cand = col[cid]  # [m, cap, 3]
+                valid = slot[None, :] < n[:, None]
+                dd = cand[:, :, :2] - pts[bb, None, :2]
+                for a in range(2):
+                    if periodic[a]:
+                        dd[..., a] -= box[a] * np.round(dd[..., a] / box[a])
+                q = (dd ** 2).sum(-1)
+                hit = valid & (q < r2)
+                if hit.any():
+                    mm, ss = np.nonzero(hit)
+                    h = np.sqrt(r2 - q[mm, ss])
+                    z0 = cand[mm, ss, 2] - rel[bb[mm], 2]
+                    iv = np.stack([z0 - h, z0 + h], axis=1)
+                    if periodic[2]:
+                        iv = np.concatenate([iv, iv - box[2], iv + box[2]])
+                    iv = iv[np.argsort(iv[:, 0], kind="stable")]
+                    free = []
+                    cur = lo
+                    for a0, a1 in iv.tolist():
+                        if a0 > cur:
+                            free.append((cur, min(a0, hi)))
+                        cur = max(cur, a1)
+                        if cur >= hi:
+                            break
+                    if cur < hi:
+                        free.append((cur, hi))
+                    free = [(a, b) for a, b in free if b > a]
+                    if not free:
+                        continue
+                    lens = np.array([b - a for a, b in free])
+                    k = rng.choice(len(free), p=lens / lens.sum())
+                    zc = rng.uniform(*free[k])
+            if zc is None:
                 zc = rng.uniform(lo, hi)
             pts[:, 2] = zc + rel[:, 2]
             break
@@ -186,14 +193,14 @@ def _place_separated(rng, n_fibres, beads, box, periodic, zlo, zhi, tilt_deg, or
         for a in range(3):
             if periodic[a]:
                 wp[:, a] %= box[a]
-        jx = np.minimum(np.floor(wp[:, 0] / cw[0]).astype(np.int64), ncx - 1)
-        jy = np.minimum(np.floor(wp[:, 1] / cw[1]).astype(np.int64), ncy - 1)
-        for b in range(beads):
-            n = coln[jx[b], jy[b]]
+        cx = np.minimum(np.floor(wp[:, 0] / cw[0]).astype(np.int64), ncx - 1)
+        cy = np.minimum(np.floor(wp[:, 1] / cw[1]).astype(np.int64), ncy - 1)
+        for b, cb in enumerate((cx * ncy + cy).tolist()):
+            n = coln[cb]
             if n >= cap:
                 raise RuntimeError("placement column overflow")
-            col[jx[b], jy[b], n] = wp[b]
-            coln[jx[b], jy[b]] = n + 1
+            col[cb, n] = wp[b]
+            coln[cb] = n + 1
     return out
 
 
@@ -280,16 +287,17 @@ def tensile_network(seed=1, fibres=20000, beads=50, box=(1000.0, 1000.0, 20.0),
                     z_range=(1.0, 19.0), k_s=100.0, young=1e3, fail_mu=math.log(5.0),
                     fail_sigma=0.3, k_a=10.0, lj_eps=1.0, lj_sigma=1.0, lj_cut=2.5, dt=0.0005,
                     clamp_lo=2.0, clamp_hi=998.0, pull=0.01, cell=2.5, wall_k=100.0,
-                    min_sep=1.0, grid_update_freq=8) -> Model:
+                    min_sep=1.0, grid_update_freq=8, placement="native") -> Model:
     """Tensile test (config 1 at its default sizes): finite in x and z,
     periodic in y; HR_FL springs with E = 1e3 and lognormal failure stress;
     LJ contacts (eps 1, sigma 1, cut-off 2.5); beads with x < 2 clamped, beads
     with x > 998 pulled at +0.01 in x.  Fibres are placed at least ``min_sep``
     apart so the LJ core starts bounded.  Bead types: C1 free, CL left clamp,
-    CR right clamp (mass 0)."""
+    CR right clamp (mass 0).  ``placement``: see place_fibres."""
     rng = np.random.default_rng(seed)
     periodic = (False, True, False)
-    pts = place_fibres(rng, fibres, beads, box, periodic, z_range=z_range, min_sep=min_sep)
+    pts = place_fibres(rng, fibres, beads, box, periodic, z_range=z_range, min_sep=min_sep,
+                       placement=placement)
     N = fibres * beads
     img = pts.reshape(N, 3)
     bt = np.zeros(N, np.int32)

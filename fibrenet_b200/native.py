@@ -119,6 +119,9 @@ SIGNATURES = {
     "fn_get_permutation": (C.c_int, [C.c_void_p, _I]),
     "fn_forces_only": (C.c_int, [C.c_void_p, C.c_int]),
     "fn_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "fn_state_save": (C.c_int, [C.c_void_p]),
+    "fn_state_restore": (C.c_int, [C.c_void_p]),
+    "fn_step_timed": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "fn_enable_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "fn_kernel_time": (C.c_int, [C.c_void_p, _D, C.POINTER(C.c_longlong), _D,
                                  C.POINTER(C.c_longlong)]),
@@ -248,6 +251,21 @@ class Simulation:
     # --- stepping
     def step(self, n: int):
         self._check(self.lib.fn_step(self.h, int(n)))
+
+    def step_timed(self, n: int) -> float:
+        """fn_step(n) timed with CUDA events on the context's stream; returns
+        the device time in ms (waits for the steps)."""
+        ms = C.c_double()
+        self._check(self.lib.fn_step_timed(self.h, int(n), C.byref(ms)))
+        return ms.value
+
+    def save_state(self):
+        """Device-side snapshot of the dynamic state (fn_state_save)."""
+        self._check(self.lib.fn_state_save(self.h))
+
+    def restore_state(self):
+        """Puts the last snapshot back (fn_state_restore)."""
+        self._check(self.lib.fn_state_restore(self.h))
 
     def rebuild(self):
         self._check(self.lib.fn_rebuild_contacts(self.h))

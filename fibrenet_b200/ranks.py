@@ -51,3 +51,28 @@ def job_rate(units_this_rank: float, elapsed_ms_this_rank: float, dist=None, dev
     units = total(units_this_rank, dist, device)
     ms = slowest(elapsed_ms_this_rank, dist, device)
     return units / (ms / 1e3)
+
+
+def gather_networks(local_indices, local_rows, n_networks: int, dist=None):
+    """All-gather of per-network results of a partitioned ensemble: rank r
+    holds the rows (one array per network, any shape) of the networks
+    ``local_indices``; every rank receives the list of all n_networks rows in
+    network order.  Without a process group the local rows are the whole."""
+    import numpy as np
+    rows = [np.asarray(x) for x in local_rows]
+    if len(rows) != len(local_indices):
+        raise ValueError("one row per local network")
+    pieces = [(list(local_indices), rows)]
+    if dist is not None and dist.is_initialized():
+        pieces = [None] * dist.get_world_size()
+        dist.all_gather_object(pieces, (list(local_indices), rows))
+    out = [None] * n_networks
+    for idx, rs in pieces:
+        for i, r in zip(idx, rs):
+            if out[i] is not None:
+                raise ValueError(f"network {i} reported by two ranks")
+            out[i] = r
+    missing = [i for i, r in enumerate(out) if r is None]
+    if missing:
+        raise ValueError(f"networks {missing[:5]} reported by no rank")
+    return out

@@ -304,12 +304,15 @@ FN_API int fn_step_series(fn_ctx* ctx, int nsteps, int every, int net, int react
    {reaction x, y, z, broken springs, dead angles} as 5 doubles to the
    caller's device buffer out_device, asynchronously on the context's stream
    (read it after fn_sync).  Calls no cudaMalloc/cudaFree: its scratch is a
-   fixed 320 KB array in the library, which every GPU that loads the library
-   keeps until exit.  Networks with more than 2,097,152 beads, springs or
-   angles are rejected with FN_ERR_CAPACITY (use fn_observe).  The first call
-   on a device looks up the scratch's device address; make it before any
-   stream capture.  All calls share the scratch: calls that overlap on the GPU
-   (other streams or contexts on the same device) race. */
+   fixed 40 KB array in the library (1,024 partial sums, the most that
+   fn_observe's reduction uses; larger networks loop inside each block), which
+   every GPU that loads the library keeps until exit.  Results equal
+   fn_observe's bit for bit at every network size; a reduction that would need
+   more partial sums than the array holds is rejected with FN_ERR_CAPACITY.
+   The first call on a device looks up the scratch's device address; make it
+   before any stream capture, and do not call it on a device after a
+   cudaDeviceReset.  All calls share the scratch: calls that overlap on the
+   GPU (other streams or contexts on the same device) race. */
 FN_API int fn_observe_noalloc(fn_ctx* ctx, int net, int reaction_type, double* out_device);
 
 /* Grid and contact-list inspection (tests): cell of each bead (-1 outside
@@ -339,6 +342,21 @@ FN_API int fn_device_view(fn_ctx* ctx, int field, fn_view* out);
    one snapshot of the state, restored after every trial, and keeps the
    fastest; the simulation does not advance. */
 FN_API int fn_autotune(fn_ctx* ctx, int steps_per_trial);
+
+/* Device-side snapshot of the dynamic state (positions, images, velocities,
+   forces, bond statuses, counters; in displacement mode also the reference
+   images and the rebuild gate), kept in one device buffer of the context.
+   fn_state_restore puts the last snapshot back (the step count with it), so
+   the same steps can be run again from the same state; a new fn_upload drops
+   the snapshot.  No counterpart in the reference, whose restart files
+   (SimulationManager.cpp:1739-1884) go through the host: fn_download /
+   fn_set_beads / fn_set_status remain the file path. */
+FN_API int fn_state_save(fn_ctx* ctx);
+FN_API int fn_state_restore(fn_ctx* ctx);
+
+/* fn_step bracketed by CUDA events on the context's stream: waits for the
+   steps to finish and writes their device time (ms) to *ms. */
+FN_API int fn_step_timed(fn_ctx* ctx, int nsteps, double* ms);
 
 /* Average duration (ms) of the step kernel over the last fn_step call when
    timing is enabled, with the launch count. */

@@ -22,7 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libfnoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfnref.so")
-REF_SRC_DEFAULT = "/root/reference/FibreNet"
+REF_SRC_ENV = "FIBRENET_REF_SRC"  # the reference's FibreNet folder (holding kernel.cl)
 
 MODE_REF = 0
 MODE_MIRROR = 1
@@ -52,12 +52,16 @@ class FoModel(C.Structure):
 
 
 def build(ref_src: str | None = None, quiet: bool = True) -> None:
-    """Builds the restatement (always) and the reference copy (when the
-    reference tree is present)."""
+    """Builds the restatement (always) and the reference copy when the
+    reference's FibreNet folder is given (``ref_src`` or the FIBRENET_REF_SRC
+    environment variable); without it an already built copy is kept."""
     env = dict(os.environ)
     targets = ["oracle"]
-    src = ref_src or REF_SRC_DEFAULT
-    if os.path.isfile(os.path.join(src, "kernel.cl")):
+    src = ref_src or os.environ.get(REF_SRC_ENV)
+    if src:
+        if not os.path.isfile(os.path.join(src, "kernel.cl")):
+            raise RuntimeError(f"{REF_SRC_ENV}={src}: no kernel.cl there (give the reference's "
+                               "FibreNet folder)")
         targets.append("ref")
         env["REF_SRC"] = src
     out = subprocess.run(["make", "-C", HERE, *targets], env=env, capture_output=True, text=True)

@@ -5,7 +5,7 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-from fibrenet_b200.ranks import job_rate, partition_networks, slowest
+from fibrenet_b200.ranks import gather_networks, job_rate, partition_networks, slowest
 
 
 def test_partition_balances_and_covers():
@@ -98,3 +98,44 @@ def test_rank_that_leaves_ends_the_others_collective_with_an_error():
     what, waited = out[0]
     assert what != "no error"
     assert waited < 60.0
+
+
+def _worker_gather(rank, world, port, out):
+    import numpy as np
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        counts = [500, 4000, 1200, 3000, 800, 2500, 100]
+        mine = partition_networks(counts, world)[rank]
+        # every network's "curve" is a function of its index alone
+        rows = [np.full((3, 2), 10.0 * i + 0.5) for i in mine]
+        allrows = gather_networks(mine, rows, len(counts), dist)
+        out[rank] = [float(r[0, 0]) for r in allrows]
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_networks_over_two_gloo_ranks():
+    """Per-network results of a partitioned ensemble come back to every rank
+    in network order."""
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_gather, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    want = [10.0 * i + 0.5 for i in range(7)]
+    assert out[0] == out[1] == want
+
+
+def test_gather_networks_rejects_gaps_and_duplicates():
+    import numpy as np
+    with pytest.raises(ValueError):
+        gather_networks([0, 2], [np.zeros(1), np.zeros(1)], 3)
+    assert [float(x[0]) for x in gather_networks([1, 0], [np.ones(1), np.zeros(1)], 2)] == [0.0, 1.0]

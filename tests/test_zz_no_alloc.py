@@ -39,8 +39,40 @@ def test_observe_noalloc_matches_observe():
             assert torch.cuda.mem_get_info()[0] == free_before
             for out in outs:
                 got = out.cpu().numpy()
-                np.testing.assert_allclose(got[:3], want["reaction"], rtol=1e-12, atol=1e-12)
+                np.testing.assert_array_equal(got[:3], want["reaction"])  # same partial sums
                 assert int(got[3]) == want["broken"]
                 assert int(got[4]) == want["angles_dead"]
             broke_seen |= want["broken"] > 0
         assert broke_seen
+
+
+def test_observe_noalloc_large_network_bit_identical():
+    """A 375,000-bead network: its reduction needs more than 1,024 blocks'
+    worth of items, so both entry points loop inside their 1,024 blocks and
+    must still agree bit for bit, call after call."""
+    import torch
+
+    from fibrenet_b200 import generate as g
+    from fibrenet_b200.native import Simulation
+
+    F = 7500
+    side = 1000.0 * np.sqrt(F / 20000.0)
+    m = g.tensile_network(seed=9, fibres=F, box=(side, side, 20.0), clamp_lo=2.0, clamp_hi=side - 2.0,
+                          pull=0.5, fail_mu=np.log(0.5), fail_sigma=0.4)
+    assert m.n_beads > 1024 * 256
+    with Simulation(m, list_capacity=64) as s:
+        out = torch.full((5,), -1.0, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            s.step(40)
+            want = s.observe(0, reaction_type=2)
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
+            s.observe_noalloc(out.data_ptr(), 0, reaction_type=2)
+            s.observe_noalloc(out.data_ptr(), 0, reaction_type=2)
+            s.sync()
+            assert torch.cuda.mem_get_info()[0] == free_before
+            got = out.cpu().numpy()
+            np.testing.assert_array_equal(got[:3], want["reaction"])
+            assert int(got[3]) == want["broken"]
+            assert int(got[4]) == want["angles_dead"]
+        assert want["broken"] > 0
