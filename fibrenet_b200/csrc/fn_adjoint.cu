@@ -662,13 +662,7 @@ int load_checkpoint(fn_ctx* c, int slot) {
 }
 
 int launch_step_args(fn_ctx* c, const fn::StepArgs& A, bool do_drift, bool store_v) {
-    if (c->chain)
-        CK(fn::launch_step_chain(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
-    else if (c->tiled)
-        CK(fn::launch_step_tiled(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
-    else
-        CK(fn::launch_step(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
-    return FN_OK;
+    return launch_step_kernel(c, A, do_drift, store_v);
 }
 
 int rebuild_from(fn_ctx* c, const double4* pos) {

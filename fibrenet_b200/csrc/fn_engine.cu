@@ -36,6 +36,10 @@ using fnh::NetHost;
 
 namespace {
 
+/* contact items per thread and round of the staged chain kernel at upload
+   (fn_autotune may pick another) */
+constexpr int kDefaultItemsPerThread = 4;
+
 /* Largest listing radius squared of one network (kernel.cl:632-650): the
    cutoff for lj/st pairs, largest radius + largest skin for hs pairs. */
 double list_r2(const NetHost& h, double cutoff_sq, double smax) {
@@ -180,6 +184,8 @@ void free_all(fn_ctx* c) {
     dfree(c, c->ch_an);
     dfree(c, c->ch_flags);
     dfree(c, c->ch_status);
+    dfree(c, c->csr);
+    dfree(c, c->tile_items);
     dfree(c, c->tile_sp_off);
     dfree(c, c->tile_sp);
     dfree(c, c->tile_an_off);
@@ -683,10 +689,16 @@ int ensure_incidence(fn_ctx* c) {
     return FN_OK;
 }
 
-int set_block(fn_ctx* c, int block) {
+/* Block size (and, for the staged chain kernel, contact items per thread and
+   round) of the step kernel: tiles, per-tile tables and kernel attributes.
+   items_per_thread 0 selects the plain chain kernel. */
+int set_block(fn_ctx* c, int block, int items_per_thread) {
     if (c->chain && block > fn::kChainMaxBlock)
         return fail(c, FN_ERR_ARG, "block size " + std::to_string(block) + ": the chain step kernel takes at most " +
                                        std::to_string(fn::kChainMaxBlock) + " threads per block");
+    if (items_per_thread < 0 || items_per_thread > fn::kStagedMaxItemsPerThread)
+        return fail(c, FN_ERR_ARG, "contact items per thread must be 0 .. " +
+                                       std::to_string(fn::kStagedMaxItemsPerThread));
     drop_graphs(c);
     std::vector<FnTile> t;
     /* the chain kernel stages its tile plus a two-bead halo on each side:
@@ -698,6 +710,27 @@ int set_block(fn_ctx* c, int block) {
     CK(h2d(c, c->tiles, t));
     if (c->chain) {
         CK(fn::prepare_step_chain(fn::step_chain_smem(block)));
+        c->staged = items_per_thread > 0;
+        c->chunk = items_per_thread * block;
+        if (c->staged) {
+            const size_t smem = fn::step_staged_smem(block, c->chunk);
+            int dev = 0, optin = 0;
+            CK(cudaGetDevice(&dev));
+            CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            if (smem > (size_t)optin)
+                return fail(c, FN_ERR_ARG, "staged step kernel: " + std::to_string(smem) +
+                                               " bytes of shared memory per block exceed the device's " +
+                                               std::to_string(optin));
+            CK(fn::prepare_step_staged(smem));
+            /* region per tile: every bead's full list, in whole 16-byte units */
+            c->csr_region = ((long long)(block - 4) * c->cfg.list_capacity + 3) / 4 * 4;
+            CK(dalloc(c, c->csr, (size_t)n * (size_t)c->csr_region + 16));
+            CK(dalloc(c, c->tile_items, (size_t)n));
+            CK(cudaMemsetAsync(c->tile_items.p, 0, sizeof(int) * (size_t)n, c->stream));
+        } else {
+            dfree(c, c->csr);
+            dfree(c, c->tile_items);
+        }
     } else {
         int r = ensure_incidence(c);
         if (r) return r;
@@ -707,6 +740,18 @@ int set_block(fn_ctx* c, int block) {
     CK(cudaStreamSynchronize(c->stream));
     c->ntiles = n;
     c->block = block;
+    return FN_OK;
+}
+
+int launch_step_kernel(fn_ctx* c, const fn::StepArgs& A, bool do_drift, bool store_v) {
+    if (c->chain && c->staged)
+        CK(fn::launch_step_staged(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    else if (c->chain)
+        CK(fn::launch_step_chain(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    else if (c->tiled)
+        CK(fn::launch_step_tiled(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    else
+        CK(fn::launch_step(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
     return FN_OK;
 }
 
@@ -753,6 +798,10 @@ fn::StepArgs step_args(fn_ctx* c, bool pingpong) {
     A.ch_flags = c->ch_flags.p;
     A.ch_status = c->ch_status.p;
     A.nb = (int)c->nb;
+    A.csr = c->csr.p;
+    A.csr_region = c->csr_region;
+    A.tile_items = c->tile_items.p;
+    A.chunk = c->chunk;
     return A;
 }
 
@@ -776,6 +825,9 @@ fn::RebuildArgs rebuild_args(fn_ctx* c) {
     R.cell_cap = c->cfg.cell_capacity;
     R.counters = c->counters.p;
     R.n_nets = c->n_nets;
+    R.csr = c->staged ? c->csr.p : nullptr;
+    R.csr_region = c->csr_region;
+    R.tile_items = c->tile_items.p;
     return R;
 }
 
@@ -818,12 +870,8 @@ int launch_one_step(fn_ctx* c, bool do_drift, bool store_v) {
         e1 = next_event(c);
         CK(cudaEventRecord(e0, c->stream));
     }
-    if (c->chain)
-        CK(fn::launch_step_chain(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
-    else if (c->tiled)
-        CK(fn::launch_step_tiled(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
-    else
-        CK(fn::launch_step(A, c->ntiles, c->block, c->damp, do_drift, store_v, c->stream));
+    int r = launch_step_kernel(c, A, do_drift, store_v);
+    if (r) return r;
     if (c->timing) {
         CK(cudaEventRecord(e1, c->stream));
         c->ev_step.emplace_back(e0, e1);
@@ -1298,7 +1346,8 @@ static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) 
     for (int k = 0; k < 2; ++k)
         if (copy_err[k] != cudaSuccess)
             return fail(c, FN_ERR_CUDA, copy_what[k] + ": " + cudaGetErrorString(copy_err[k]));
-    int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128);
+    int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128,
+                      c->cfg.chain_mode == 0 ? kDefaultItemsPerThread : 0);
     if (r) return r;
     r = verlet_setup(c);
     if (r) return r;
@@ -1379,8 +1428,12 @@ FN_API int fn_sync(fn_ctx* c) {
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
     if (!c->uploaded) return FN_OK;
-    unsigned long long bad = 0;
-    CK(cudaMemcpy(&bad, c->counters.p + FN_CNT_NONFINITE, sizeof bad, cudaMemcpyDeviceToHost));
+    unsigned long long cnt[FN_CNT_N];
+    CK(cudaMemcpy(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost));
+    if (cnt[FN_CNT_STALL])
+        return fail(c, FN_ERR_CUDA, "a step kernel's wait for staged data ran out in " +
+                                        std::to_string(cnt[FN_CNT_STALL]) + " tiles (the state is unusable)");
+    const unsigned long long bad = cnt[FN_CNT_NONFINITE];
     if (bad) return fail(c, FN_ERR_NONFINITE, "non-finite force detected in " + std::to_string(bad) + " bead-steps");
     return FN_OK;
     FN_CATCH(c)
@@ -1808,6 +1861,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     if (!c || !out) return FN_ERR_ARG;
     std::memset(out, 0, sizeof *out);
     out->block_size = c->block;
+    out->items_per_thread = c->staged ? c->chunk / c->block : 0;
     out->bond_path = c->chain ? 2 : (c->tiled ? 1 : 0);
     out->graph_launches = c->graph_launches;
     out->n_networks = c->n_nets;
@@ -1822,6 +1876,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     CK(cudaStreamSynchronize(c->stream));
     if (c->verlet) out->rebuilds = (long long)cnt[FN_CNT_REBUILDS];
     out->nonfinite = (long long)cnt[FN_CNT_NONFINITE];
+    out->stalls = (long long)cnt[FN_CNT_STALL];
     out->cell_overflow = (long long)cnt[FN_CNT_CELL_OVERFLOW];
     out->list_overflow = (long long)cnt[FN_CNT_LIST_OVERFLOW];
     if (cnt[FN_CNT_NONFINITE]) c->err = "non-finite force detected";
@@ -1931,10 +1986,11 @@ FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, doubl
     FN_CATCH(c)
 }
 
-/* Block-size tuner: for each candidate the same `steps_per_trial` steps run
-   from one snapshot of the state (restored after every trial, so the
-   simulation does not advance), timed with CUDA events; the fastest block
-   size is kept. */
+/* Step-kernel tuner: for each candidate shape -- block size and, for the
+   staged chain kernel, contact items per thread and round (0: the plain chain
+   kernel) -- the same `steps_per_trial` steps run from one snapshot of the
+   state (restored after every trial, so the simulation does not advance),
+   timed with CUDA events; the fastest shape is kept. */
 FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     FN_TRY
     fnh::NvtxRange nvtx_range_("fn_autotune");
@@ -1970,15 +2026,24 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     const long long steps0 = c->steps_done, rb0 = c->rebuilds_done;
     const bool timing0 = c->timing;
     c->timing = false;
-    const int candidates[] = {64, 96, 128, 192, 256, 384, 512};
-    int best = c->block;
+    std::vector<std::pair<int, int>> shapes;
+    for (int b : {64, 96, 128, 192, 256, 384, 512}) {
+        if (c->chain && b > fn::kChainMaxBlock) continue;
+        if (c->chain && c->cfg.chain_mode == 0)
+            for (int k : {2, 4, 8}) shapes.emplace_back(b, k);
+        shapes.emplace_back(b, 0);
+    }
+    int dev = 0, optin = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    std::pair<int, int> best{c->block, c->staged ? c->chunk / c->block : 0};
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    for (int b : candidates) {
-        if (c->chain && b > fn::kChainMaxBlock) continue;
-        if ((r = set_block(c, b))) break;
+    for (const auto& sh : shapes) {
+        if (sh.second > 0 && fn::step_staged_smem(sh.first, sh.first * sh.second) > (size_t)optin) continue;
+        if ((r = set_block(c, sh.first, sh.second))) break;
         for (int rep = 0; rep < 2 && !r; ++rep) { /* first run warms up */
             c->cur = cur0;
             for (auto& sn : snaps)
@@ -1993,7 +2058,7 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
         CK(cudaEventElapsedTime(&ms, e0, e1));
         if (ms < best_ms) {
             best_ms = ms;
-            best = b;
+            best = sh;
         }
     }
     cudaEventDestroy(e0);
@@ -2008,7 +2073,23 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     c->rebuilds_done = rb0;
     c->timing = timing0;
     if (r) return r;
-    return set_block(c, best);
+    return set_block(c, best.first, best.second);
+    FN_CATCH(c)
+}
+
+/* Sets the step kernel's shape directly (what fn_autotune picks). */
+FN_API int fn_set_kernel_shape(fn_ctx* c, int block, int items_per_thread) {
+    FN_TRY
+    int r = check_ready(c);
+    if (r) return r;
+    if (block < 32 || block > 512 || block % 32 != 0)
+        return fail(c, FN_ERR_ARG, "fn_set_kernel_shape: block must be a multiple of 32 in 32 .. 512");
+    if (items_per_thread != 0 && !(c->chain && c->cfg.chain_mode == 0))
+        return fail(c, FN_ERR_UNSUPPORTED, "fn_set_kernel_shape: contact staging needs the chain path (chain_mode 0)");
+    if (c->chain && block < 64) return fail(c, FN_ERR_ARG, "fn_set_kernel_shape: chain tiles need blocks of 64 or more");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    return set_block(c, block, items_per_thread);
     FN_CATCH(c)
 }
 

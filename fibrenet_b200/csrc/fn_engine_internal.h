@@ -99,6 +99,12 @@ struct fn_ctx {
     DevBuf<float4> ch_sp;
     DevBuf<float2> ch_an;
     DevBuf<unsigned char> ch_flags, ch_status;
+    /* staged chain step kernel: tile-compacted contact list, items per tile,
+       contact items staged per round */
+    bool staged = false;
+    int chunk = 0;
+    long long csr_region = 0;
+    DevBuf<int> csr, tile_items;
     DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
     DevBuf<int> scan_sums;
     DevBuf<FnTile> tiles;
@@ -216,6 +222,9 @@ void dfree(fn_ctx* c, DevBuf<T>& b) {
 int check_ready(fn_ctx* c);
 int ensure_incidence(fn_ctx* c);
 fn::StepArgs step_args(fn_ctx* c, bool pingpong);
+/* one step launch of the kernel the context uses (chain: staged or plain;
+   per-tile or per-bead incidence otherwise) */
+int launch_step_kernel(fn_ctx* c, const fn::StepArgs& A, bool do_drift, bool store_v);
 fn::RebuildArgs rebuild_args(fn_ctx* c);
 void drop_graphs(fn_ctx* c);
 

@@ -825,6 +825,344 @@ __global__ void __launch_bounds__(kChainMaxBlock, 4) k_step_chain(const StepArgs
     kick_drift_store<DAMP, DRIFT, STORE_V>(A, N, i, p, Fx, Fy, Fz);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Staged chain step kernel                                                  */
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+/* mbarrier + bulk-copy (TMA, non-tensor) primitives for one CTA */
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+/* Waits for phase `parity` of the barrier for at most ~2 s of SM clock;
+   false when the wait ran out. */
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > 4000000000LL) return false;
+    return true;
+}
+/* bytes (a multiple of 16) from global src to shared dst, both 16-byte
+   aligned, completing on the barrier */
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+/* 16 bytes global -> shared through L2 (LDGSTS) */
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
+}
+
+/* Issues the partner-position copies of contact items [c0, c0 + nch) of the
+   tile: item q's partner j (tile-compacted list) -> pj slot q - c0.  The
+   entries are loaded first, all at once, so their latency is paid once. */
+__device__ __forceinline__ void gather_partners(const StepArgs& A, const int* __restrict__ ent, int c0,
+                                                int nch, unsigned char* s_pj) {
+    int j[kStagedMaxItemsPerThread];
+#pragma unroll
+    for (int k = 0; k < kStagedMaxItemsPerThread; ++k) {
+        const int q = (int)threadIdx.x + k * (int)blockDim.x;
+        j[k] = q < nch ? ent[c0 + q] : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kStagedMaxItemsPerThread; ++k) {
+        const int q = (int)threadIdx.x + k * (int)blockDim.x;
+        if ((unsigned)j[k] < (unsigned)A.nb) {
+            const double4* src = A.pos_in + j[k];
+            const uint32_t dst = smem_addr(s_pj + 32 * (size_t)q);
+            cp_async16(dst, src);
+            cp_async16(dst + 16, reinterpret_cast<const char*>(src) + 16);
+        }
+    }
+}
+
+/* The chain step (same arithmetic and summation order as k_step_chain, so
+   the same bits) with the tile's data staged in shared memory before any of
+   it is used, instead of a chain of dependent loads:
+     - one thread issues bulk copies (cp.async.bulk, completing on an
+       mbarrier) of the image positions (with a two-bead halo each side),
+       positions, forces, velocities_old and spring records of the tile;
+     - meanwhile every thread loads the tile's contact entries (a contiguous
+       run of the tile-compacted list) and copies each partner's position
+       into shared memory (cp.async), and the byte-sized flags, statuses,
+       angle records and list lengths with plain loads;
+     - then springs and angles are evaluated once per tile, every contact
+       item is evaluated by some thread of the block (items spread evenly over
+       the threads, results kept per item), and each thread sums its bead's
+       terms in the fixed order: base, previous and next spring, angles
+       centred on j-1, j, j+1, contacts in list order.
+   Tiles with more contact items than `chunk` take them in rounds. */
+template <bool DAMP, bool DRIFT, bool STORE_V>
+__global__ void __launch_bounds__(kChainMaxBlock) k_step_staged(const StepArgs A) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const StagedSmem L = staged_smem_layout(blockDim.x, A.chunk);
+    const FnTile tile = A.tiles[blockIdx.x];
+    const int items = A.tile_items[blockIdx.x];
+    const int b0 = tile.begin, n = tile.end - tile.begin;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int* __restrict__ ent = A.csr + (size_t)blockIdx.x * (size_t)A.csr_region;
+    const uint32_t bar = smem_addr(sm + L.bar);
+    const int j0 = max(b0 - 2, 0), j1 = min(b0 + n + 2, A.nb), js1 = min(b0 + n + 1, A.nb);
+    double* s_spf = reinterpret_cast<double*>(sm + L.spf);
+    double* s_ang = reinterpret_cast<double*>(sm + L.ang);
+    const double4* s_img = reinterpret_cast<const double4*>(sm + L.img);
+    const double4* s_pos = reinterpret_cast<const double4*>(sm + L.pos);
+    const float4* s_frc = reinterpret_cast<const float4*>(sm + L.frc);
+    const float4* s_vold = reinterpret_cast<const float4*>(sm + L.vold);
+    const float4* s_chsp = reinterpret_cast<const float4*>(sm + L.chsp);
+    float2* s_chan = reinterpret_cast<float2*>(sm + L.chan);
+    unsigned char* s_pj = sm + L.pj;
+    int* s_off = reinterpret_cast<int*>(sm + L.off);
+    int* s_ws = reinterpret_cast<int*>(sm + L.ws);
+    unsigned char* s_owner = sm + L.owner;
+    unsigned char* s_flag = sm + L.flag;
+    unsigned char* s_stat = sm + L.stat;
+    unsigned char* s_tsp = sm + L.tsp;
+    unsigned char* s_tan = sm + L.tan;
+
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = 32u * (uint32_t)(j1 - j0) + 32u * (uint32_t)n + 32u * (uint32_t)n +
+                               16u * (uint32_t)(js1 - j0);
+        mbar_expect_tx(bar, bytes);
+        bulk_g2s(smem_addr(sm + L.img) + 32u * (uint32_t)(j0 - (b0 - 2)), A.img_in + j0, 32u * (j1 - j0), bar);
+        bulk_g2s(smem_addr(sm + L.pos), A.pos_in + b0, 32u * n, bar);
+        bulk_g2s(smem_addr(sm + L.frc), A.force + b0, 16u * n, bar);
+        bulk_g2s(smem_addr(sm + L.vold), A.vold + b0, 16u * n, bar);
+        bulk_g2s(smem_addr(sm + L.chsp) + 16u * (uint32_t)(j0 - (b0 - 2)), A.ch_sp + j0, 16u * (js1 - j0), bar);
+    }
+    /* the first round's contact partners, while the bulk copies run */
+    const int nch0 = min(items, A.chunk);
+    gather_partners(A, ent, 0, nch0, s_pj);
+    /* byte-sized and 8-byte arrays, list length */
+    const bool active = tid < n;
+    const int i = b0 + tid;
+    int nc = 0;
+    if (active) {
+        nc = A.list_count[i];
+        if (nc > A.list_cap) nc = A.list_cap;
+    }
+    for (int u = tid; u < n + 4; u += nt) {
+        const int j = b0 - 2 + u;
+        unsigned char fl = 0, st = 0;
+        if (j >= 0 && j < A.nb) {
+            fl = A.ch_flags[j];
+            st = A.ch_status[j];
+        }
+        s_flag[u] = fl;
+        s_stat[u] = st;
+        if (u < n + 2) {
+            const int ja = b0 - 1 + u;
+            s_chan[u] = (ja >= 0 && ja < A.nb) ? A.ch_an[ja] : make_float2(0.f, 0.f);
+        }
+    }
+    /* each bead's first contact item and the item -> bead map of round 0 */
+    int total;
+    const int off = block_scan_any(nc, s_ws, total);
+    if (tid < n) s_off[tid] = off;
+    for (int q = off; q < min(off + nc, nch0); ++q) s_owner[q] = (unsigned char)tid;
+
+    cp_async_wait_all();
+    bool ok = mbar_wait_bounded(bar, 0);
+    ok = __syncthreads_and(ok);
+    if (!ok) {
+        /* the staged data never arrived: skip the tile, counted for fn_sync */
+        if (tid == 0) {
+            atomicAdd(A.counters + FN_CNT_STALL, 1ull);
+            mbar_wait_bounded(bar, 0);
+        }
+        __syncthreads();
+        return;
+    }
+
+    /* springs: lower bead b0 - 2 + u, u < n + 3 */
+    for (int u = tid; u < n + 3; u += nt) {
+        const unsigned fl = s_flag[u];
+        unsigned char tf = 0;
+        if (fl & FN_CH_SPRING) {
+            const int alive0 = s_stat[u] & 1;
+            tf = (unsigned char)(alive0 << 2);
+            if (alive0 && !(fl & FN_CH_SP_INERT)) {
+                const double4 a = s_img[(fl & FN_CH_SP_REV) ? u + 1 : u];
+                const double4 b = s_img[(fl & FN_CH_SP_REV) ? u : u + 1];
+                double fx = 0.0, fy = 0.0, fz = 0.0;
+                int broke;
+                const int acts = spring_pts(a.x, a.y, a.z, b.x, b.y, b.z, s_chsp[u], (fl & FN_CH_SP_FL) ? 1 : 0,
+                                            fx, fy, fz, broke);
+                s_spf[3 * u] = fx;
+                s_spf[3 * u + 1] = fy;
+                s_spf[3 * u + 2] = fz;
+                tf |= (unsigned char)(acts | (broke << 1));
+            }
+        }
+        s_tsp[u] = tf;
+    }
+    __syncthreads();
+    /* angles: centre b0 - 1 + u, u < n + 2 */
+    for (int u = tid; u < n + 2; u += nt) {
+        const unsigned fl = s_flag[u + 1];
+        int alive = (fl & FN_CH_ANGLE) && (s_stat[u + 1] & 2);
+        if (alive && (fl & FN_CH_AN_FL)) {
+            const unsigned f1 = s_tsp[u], f2 = s_tsp[u + 1];
+            if (!((f1 & 4) && !(f1 & 2)) || !((f2 & 4) && !(f2 & 2))) alive = 0;
+        }
+        s_tan[u] = (unsigned char)alive;
+        if (alive) {
+            const double4 t1 = s_img[(fl & FN_CH_AN_REV) ? u + 2 : u];
+            const double4 t2 = s_img[u + 1];
+            const double4 t3 = s_img[(fl & FN_CH_AN_REV) ? u : u + 2];
+            double* o = s_ang + 6 * u;
+            angle_pts(t1.x, t1.y, t1.z, t2.x, t2.y, t2.z, t3.x, t3.y, t3.z, s_chan[u], o[0], o[1], o[2], o[3],
+                      o[4], o[5]);
+        }
+    }
+    __syncthreads();
+
+    const FnNet& N = A.nets[tile.net];
+    double4 p = make_double4(0.0, 0.0, 0.0, 0.0);
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    if (active) {
+        p = s_pos[tid];
+        base_force<DAMP>(A, N, i, p, Fx, Fy, Fz);
+        const unsigned fp = s_flag[tid + 1];
+        if ((fp & FN_CH_SPRING) && (s_tsp[tid + 1] & 1)) {
+            const double* f = s_spf + 3 * (tid + 1);
+            if (fp & FN_CH_SP_REV) {
+                Fx += f[0];
+                Fy += f[1];
+                Fz += f[2];
+            } else {
+                Fx += f[0] * -1.0;
+                Fy += f[1] * -1.0;
+                Fz += f[2] * -1.0;
+            }
+        }
+        const unsigned fn = s_flag[tid + 2];
+        if ((fn & FN_CH_SPRING) && (s_tsp[tid + 2] & 1)) {
+            const double* f = s_spf + 3 * (tid + 2);
+            if (fn & FN_CH_SP_REV) {
+                Fx += f[0] * -1.0;
+                Fy += f[1] * -1.0;
+                Fz += f[2] * -1.0;
+            } else {
+                Fx += f[0];
+                Fy += f[1];
+                Fz += f[2];
+            }
+        }
+        if (s_tan[tid]) {
+            const double* o = s_ang + 6 * tid;
+            const int k = (s_flag[tid + 1] & FN_CH_AN_REV) ? 0 : 3;
+            Fx += o[k];
+            Fy += o[k + 1];
+            Fz += o[k + 2];
+        }
+        if (s_tan[tid + 1]) {
+            const double* o = s_ang + 6 * (tid + 1);
+            Fx += -o[0] - o[3];
+            Fy += -o[1] - o[4];
+            Fz += -o[2] - o[5];
+        }
+        if (s_tan[tid + 2]) {
+            const double* o = s_ang + 6 * (tid + 2);
+            const int k = (s_flag[tid + 3] & FN_CH_AN_REV) ? 3 : 0;
+            Fx += o[k];
+            Fy += o[k + 1];
+            Fz += o[k + 2];
+        }
+    }
+
+    /* contacts, in rounds of at most `chunk` items */
+    for (int c0 = 0; c0 < items; c0 += A.chunk) {
+        const int nch = min(items - c0, A.chunk);
+        if (c0 > 0) {
+            __syncthreads(); /* the previous round's results are summed */
+            gather_partners(A, ent, c0, nch, s_pj);
+            for (int q = max(off, c0); q < min(off + nc, c0 + nch); ++q) s_owner[q - c0] = (unsigned char)tid;
+            cp_async_wait_all();
+            __syncthreads();
+        }
+        for (int q = tid; q < nch; q += nt) {
+            const int t = min((int)s_owner[q], n - 1);
+            double4* slot = reinterpret_cast<double4*>(s_pj + 32 * (size_t)q);
+            const double4 pj = *slot;
+            double Rx = 0.0, Ry = 0.0, Rz = 0.0;
+            const int acts = contact_eval(N, A.pairs, s_pos[t], pj, Rx, Ry, Rz);
+            *slot = make_double4(Rx, Ry, Rz, acts ? 1.0 : 0.0);
+        }
+        __syncthreads();
+        if (active) {
+            for (int q = max(off, c0); q < min(off + nc, c0 + nch); ++q) {
+                const double4 r = *reinterpret_cast<const double4*>(s_pj + 32 * (size_t)(q - c0));
+                if (r.w != 0.0) {
+                    Fx += r.x;
+                    Fy += r.y;
+                    Fz += r.z;
+                }
+            }
+        }
+    }
+    if (!active) return;
+
+    /* statuses after this step (kernel.cl:396-397, 278-284) */
+    const unsigned st0 = s_stat[tid + 2];
+    unsigned st = st0;
+    if ((s_tsp[tid + 2] & 2)) st &= ~1u;
+    if ((st0 & 2) && (s_flag[tid + 2] & FN_CH_ANGLE) && !s_tan[tid + 1]) st &= ~2u;
+    if (st != st0) A.ch_status[i] = (unsigned char)st;
+
+    /* AdvanceVelocity (kernel.cl:451-462) and the next AdvancePosition */
+    const float fx = (float)Fx, fy = (float)Fy, fz = (float)Fz;
+    if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicAdd(A.counters + FN_CNT_NONFINITE, 1ull);
+    double4 im = s_img[tid + 2];
+    const double minv = im.w;
+    const double half_dt = N.half_dt * minv;
+    const float4 fo = s_frc[tid];
+    const float4 vo = s_vold[tid];
+    double tx = (double)fx, ty = (double)fy, tz = (double)fz;
+    tx += (double)fo.x;
+    ty += (double)fo.y;
+    tz += (double)fo.z;
+    const float vox = (float)(tx * half_dt + (double)vo.x);
+    const float voy = (float)(ty * half_dt + (double)vo.y);
+    const float voz = (float)(tz * half_dt + (double)vo.z);
+    A.force[i] = make_float4(fx, fy, fz, 0.0f);
+    A.vold[i] = make_float4(vox, voy, voz, 0.0f);
+    if (DRIFT) {
+        float4 v;
+        drift(N, minv, fx, fy, fz, vox, voy, voz, p, im, v);
+        A.pos_out[i] = p;
+        A.img_out[i] = im;
+        if (DAMP || STORE_V) A.vel[i] = v;
+    }
+}
+
 template <bool STORE_V>
 __global__ void __launch_bounds__(512) k_drift(const StepArgs A) {
     const FnTile t = A.tiles[blockIdx.x];
@@ -1104,6 +1442,27 @@ __global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long lon
     R.list_count[i] = n;
 }
 
+/* Tile-compacted copy of the contact list for the staged step kernel: tile
+   t's entries, bead after bead and in list order within a bead, from
+   csr + t * region (region >= beads per tile x list capacity), and their
+   number in tile_items[t].  One block of at least the tile's bead count. */
+__global__ void k_list_tiles(const RebuildArgs R) {
+    FN_GATED(R.gate);
+    __shared__ int ws[33];
+    const FnTile t = R.tiles[blockIdx.x];
+    const int i = t.begin + (int)threadIdx.x;
+    int c = 0;
+    if (i < t.end) {
+        c = R.list_count[i];
+        if (c > R.list_cap) c = R.list_cap;
+    }
+    int total;
+    const int off = block_scan_any(c, ws, total);
+    int* out = R.csr + (size_t)blockIdx.x * (size_t)R.csr_region + off;
+    for (int k = 0; k < c; ++k) out[k] = R.list[(size_t)k * R.list_stride + i];
+    if (threadIdx.x == 0) R.tile_items[blockIdx.x] = total;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Exclusive scan of int counts (1024 threads x 2 items per block).          */
 
@@ -1373,6 +1732,46 @@ cudaError_t launch_step_chain(const StepArgs& A, int ntiles, int block, bool dam
     return cudaGetLastError();
 }
 
+template <bool DAMP, bool DRIFT, bool STORE_V>
+static cudaError_t set_staged_smem(size_t bytes) {
+    return cudaFuncSetAttribute(k_step_staged<DAMP, DRIFT, STORE_V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bytes);
+}
+
+cudaError_t prepare_step_staged(size_t bytes) {
+    static size_t done[64] = {};
+    if (!raise_limit(done, bytes)) return cudaSuccess;
+    cudaError_t e;
+    if ((e = set_staged_smem<true, true, true>(bytes))) return e;
+    if ((e = set_staged_smem<true, false, false>(bytes))) return e;
+    if ((e = set_staged_smem<false, true, true>(bytes))) return e;
+    if ((e = set_staged_smem<false, true, false>(bytes))) return e;
+    return set_staged_smem<false, false, false>(bytes);
+}
+
+cudaError_t launch_step_staged(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
+                               bool store_v, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    const size_t sm = step_staged_smem(block, A.chunk);
+    if (damp) {
+        if (do_drift)
+            k_step_staged<true, true, true><<<ntiles, block, sm, s>>>(A);
+        else
+            k_step_staged<true, false, false><<<ntiles, block, sm, s>>>(A);
+    } else {
+        if (do_drift) {
+            if (store_v)
+                k_step_staged<false, true, true><<<ntiles, block, sm, s>>>(A);
+            else
+                k_step_staged<false, true, false><<<ntiles, block, sm, s>>>(A);
+        } else {
+            k_step_staged<false, false, false><<<ntiles, block, sm, s>>>(A);
+        }
+    }
+    return cudaGetLastError();
+}
+
+
 cudaError_t launch_forces_chain(const StepArgs& A, int ntiles, int block, int terms, cudaStream_t s) {
     if (ntiles <= 0) return cudaSuccess;
     k_step_chain<false, false, false, true><<<ntiles, block, step_chain_smem(block), s>>>(A, terms);
@@ -1429,6 +1828,9 @@ cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, 
     }
     /* every bead may sit in the grid; threads past the grid total return */
     if (nb > 0) k_lists<<<(nb + 127) / 128, 128, 0, s>>>(R, ncells);
+    /* the staged step kernel's copy, one block per tile (tiles are at most
+       block - 4 beads wide) */
+    if (R.csr && ntiles > 0) k_list_tiles<<<ntiles, block, 0, s>>>(R);
     return cudaGetLastError();
 }
 

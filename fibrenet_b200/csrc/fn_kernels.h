@@ -61,6 +61,13 @@ struct StepArgs {
     const unsigned char* ch_flags; /* FN_CH_* bits */
     unsigned char* ch_status;     /* bit 0 spring (j, j+1) alive, bit 1 angle alive */
     int nb;
+    /* tile-compacted contact list (staged step kernel): the entries of tile
+       t's beads, bead after bead in list order, from csr + t * csr_region;
+       tile_items[t] of them */
+    const int* csr;
+    long long csr_region;
+    const int* tile_items;
+    int chunk; /* contact items staged per round (a multiple of the block size) */
 };
 
 /* dynamic shared memory of the tiled step kernel */
@@ -124,6 +131,63 @@ __host__ __device__ inline ChainSmem chain_smem_layout(int block) {
 
 inline size_t step_chain_smem(int block) { return chain_smem_layout(block).total; }
 
+/* The staged chain step kernel: largest number of contact items one thread
+   gathers per round (chunk <= kStagedMaxItemsPerThread * block). */
+constexpr int kStagedMaxItemsPerThread = 8;
+
+/* Byte offsets of the staged step kernel's dynamic shared memory for blocks
+   of `block` threads (tiles of block - 4 beads) and `chunk` contact items per
+   round. */
+struct StagedSmem {
+    size_t bar, img, pos, frc, vold, chsp, chan, spf, ang, pj, off, ws, owner, flag, stat, tsp, tan,
+        total;
+};
+
+__host__ __device__ inline StagedSmem staged_smem_layout(int block, int chunk) {
+    StagedSmem L;
+    const size_t w = (size_t)block - 4, h = w + 4;
+    size_t o = 0;
+    L.bar = o;   /* mbarrier of the bulk copies */
+    o += 16;
+    L.img = o;   /* double4 image positions, slot u <-> bead b0 - 2 + u */
+    o += 32 * h;
+    L.pos = o;   /* double4 own positions */
+    o += 32 * w;
+    L.frc = o;   /* float4 force of the last step */
+    o += 16 * w;
+    L.vold = o;  /* float4 velocity_old */
+    o += 16 * w;
+    L.chsp = o;  /* float4 spring records, slot u <-> lower bead b0 - 2 + u */
+    o += 16 * h;
+    L.chan = o;  /* float2 angle records, slot u <-> centre b0 - 1 + u */
+    o += 8 * h;
+    o = smem_align(o, 16);
+    L.spf = o;   /* spring forces */
+    o += 24 * h;
+    L.ang = o;   /* angle pa, pc */
+    o += 48 * h;
+    L.pj = o;    /* per item: partner position, then (R, acts) */
+    o += 32 * (size_t)chunk;
+    L.off = o;   /* per bead: first item */
+    o += 4 * ((size_t)block + 1);
+    L.ws = o;    /* block scan */
+    o += 4 * 33;
+    L.owner = o; /* per item: local bead */
+    o += (size_t)chunk;
+    L.flag = o;
+    o += h;
+    L.stat = o;
+    o += h;
+    L.tsp = o;
+    o += h;
+    L.tan = o;
+    o += h;
+    L.total = smem_align(o, 16);
+    return L;
+}
+
+inline size_t step_staged_smem(int block, int chunk) { return staged_smem_layout(block, chunk).total; }
+
 struct RebuildArgs {
     const FnTile* tiles;
     const FnNet* nets;
@@ -143,6 +207,10 @@ struct RebuildArgs {
     unsigned long long* counters;
     int n_nets;
     const int* gate; /* displacement mode: rebuild only when *gate != 0 */
+    /* tile-compacted copy of the list for the staged step kernel (null: none) */
+    int* csr;
+    long long csr_region;
+    int* tile_items;
 };
 
 struct ObserveArgs {
@@ -202,6 +270,9 @@ cudaError_t launch_step_chain(const StepArgs& A, int ntiles, int block, bool dam
                               bool store_v, cudaStream_t s);
 cudaError_t launch_forces_chain(const StepArgs& A, int ntiles, int block, int terms, cudaStream_t s);
 cudaError_t prepare_step_chain(size_t smem_bytes);
+cudaError_t launch_step_staged(const StepArgs& A, int ntiles, int block, bool damp, bool do_drift,
+                               bool store_v, cudaStream_t s);
+cudaError_t prepare_step_staged(size_t smem_bytes);
 cudaError_t launch_drift(const StepArgs& A, int ntiles, int block, bool store_v, cudaStream_t s);
 cudaError_t launch_forces_only(const StepArgs& A, int ntiles, int block, int terms, cudaStream_t s);
 cudaError_t launch_reset_energy(float4* force, float4* vel, float4* vold, int n, cudaStream_t s);

@@ -56,6 +56,7 @@ struct FnTile {
 
 /* Device counters (unsigned long long). */
 enum { FN_CNT_CELL_OVERFLOW = 0, FN_CNT_LIST_OVERFLOW = 1, FN_CNT_NONFINITE = 2, FN_CNT_REBUILDS = 3,
-       FN_CNT_N = 4 };
+       FN_CNT_STALL = 4, /* a bounded wait on staged data ran out (the tile was skipped) */
+       FN_CNT_N = 5 };
 
 #endif

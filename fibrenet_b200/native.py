@@ -55,7 +55,8 @@ class FnStats(C.Structure):
                 ("rebuilds", C.c_longlong), ("steps", C.c_longlong), ("block_size", C.c_int),
                 ("bond_path", C.c_int), ("n_networks", C.c_int), ("n_beads", C.c_longlong),
                 ("device_bytes", C.c_longlong), ("graph_launches", C.c_longlong),
-                ("nonfinite", C.c_longlong)]
+                ("nonfinite", C.c_longlong), ("items_per_thread", C.c_int),
+                ("stalls", C.c_longlong)]
 
 
 class FnView(C.Structure):
@@ -119,6 +120,7 @@ SIGNATURES = {
     "fn_get_permutation": (C.c_int, [C.c_void_p, _I]),
     "fn_forces_only": (C.c_int, [C.c_void_p, C.c_int]),
     "fn_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "fn_set_kernel_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "fn_state_save": (C.c_int, [C.c_void_p]),
     "fn_state_restore": (C.c_int, [C.c_void_p]),
     "fn_step_timed": (C.c_int, [C.c_void_p, C.c_int, _D]),
@@ -207,11 +209,12 @@ class Simulation:
 
     def __init__(self, models, device: int = 0, cell_capacity: int = 64, list_capacity: int = 64,
                  reorder: bool = True, use_graphs: bool = False, block_size: int = 0,
-                 chain: bool = True, verlet_skin: float = 0.0):
+                 chain: bool = True, verlet_skin: float = 0.0, staged: bool = True):
         self.lib = load()
         self.models = [models] if isinstance(models, Model) else list(models)
+        chain_mode = (0 if staged else 1) if chain else 2
         cfg = FnConfig(device, cell_capacity, list_capacity, int(reorder), int(use_graphs),
-                       block_size, 0 if chain else 2, float(verlet_skin))
+                       block_size, chain_mode, float(verlet_skin))
         h = C.c_void_p()
         rc = self.lib.fn_create(C.byref(cfg), C.byref(h))
         if rc != FN_OK:
@@ -434,6 +437,11 @@ class Simulation:
         self._check(self.lib.fn_kernel_time(self.h, C.byref(ms), C.byref(n), C.byref(rms), C.byref(rn)))
         return {"step_ms": ms.value, "launches": n.value, "rebuild_ms": rms.value,
                 "rebuilds": rn.value}
+
+    def set_kernel_shape(self, block: int, items_per_thread: int = 0) -> None:
+        """Step-kernel shape: block size and, for the staged chain kernel,
+        contact items per thread and round (0: no staging)."""
+        self._check(self.lib.fn_set_kernel_shape(self.h, int(block), int(items_per_thread)))
 
     def autotune(self, steps_per_trial: int = 20) -> int:
         self._check(self.lib.fn_autotune(self.h, steps_per_trial))

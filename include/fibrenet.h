@@ -117,7 +117,9 @@ typedef struct fn_config {
     int block_size;     /* threads per block for the step kernel; 0 = default
                            (128); at most 256 on the chain path */
     int chain_mode;     /* 0 auto: per-bead bond records when the model is in
-                           chain form (fibres); 2 never (incidence lists) */
+                           chain form (fibres), the tile's data staged in
+                           shared memory before use; 1 chain form without
+                           staging; 2 never (incidence lists) */
     double verlet_skin; /* 0: the reference's cadence (rebuild every
                            grid_update_freq steps, counter local to each
                            fn_step call, SimulationManager.cpp:152-173).
@@ -144,6 +146,10 @@ typedef struct fn_stats {
     long long device_bytes;    /* device memory held by the context */
     long long graph_launches;  /* step segments replayed as CUDA graphs */
     long long nonfinite;       /* bead-steps whose new force was NaN or inf */
+    int items_per_thread;      /* staged chain kernel: contact items per thread
+                                  and round (0: another step kernel) */
+    long long stalls;          /* tiles skipped because a bounded wait for their
+                                  staged data ran out (fn_sync then fails) */
 } fn_stats;
 
 /* A device array of the context, for zero-copy readers (torch through
@@ -338,10 +344,19 @@ FN_API int fn_get_permutation(fn_ctx* ctx, int* perm);
    FN_VELOCITY_OLD) without a copy; synchronises the context's stream first. */
 FN_API int fn_device_view(fn_ctx* ctx, int field, fn_view* out);
 
-/* Times steps_per_trial steps at each candidate block size (64 .. 512) from
-   one snapshot of the state, restored after every trial, and keeps the
-   fastest; the simulation does not advance. */
+/* Times steps_per_trial steps at each candidate shape of the step kernel
+   (block size 64 .. 512; for the staged chain kernel also 2, 4 or 8 contact
+   items per thread and round, or no staging) from one snapshot of the state,
+   restored after every trial, and keeps the fastest; the simulation does not
+   advance. */
 FN_API int fn_autotune(fn_ctx* ctx, int steps_per_trial);
+
+/* Sets the step kernel's shape: threads per block (a multiple of 32; 64 ..
+   256 on the chain path, whose tiles hold block - 4 beads) and, for the
+   staged chain kernel (chain_mode 0), contact items per thread and round
+   (1 .. 8; 0 runs the chain kernel without staging).  fn_autotune picks the
+   same parameters by timing. */
+FN_API int fn_set_kernel_shape(fn_ctx* ctx, int block, int items_per_thread);
 
 /* Device-side snapshot of the dynamic state (positions, images, velocities,
    forces, bond statuses, counters; in displacement mode also the reference

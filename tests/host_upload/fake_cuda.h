@@ -36,6 +36,14 @@ static inline cudaError_t hu_count(int* n) {
     *n = 1;
     return cudaSuccess;
 }
+static inline cudaError_t hu_device(int* d) {
+    *d = 0;
+    return cudaSuccess;
+}
+static inline cudaError_t hu_attr(int* v) {
+    *v = 227 * 1024; /* a B200's opt-in shared memory per block */
+    return cudaSuccess;
+}
 static inline cudaError_t hu_stream(cudaStream_t* s) {
     *s = nullptr;
     return cudaSuccess;
@@ -43,6 +51,8 @@ static inline cudaError_t hu_stream(cudaStream_t* s) {
 
 #define cudaSetDevice(d) hu_ok()
 #define cudaGetDeviceCount(n) hu_count(n)
+#define cudaGetDevice(d) hu_device(d)
+#define cudaDeviceGetAttribute(v, a, d) hu_attr(v)
 #define cudaStreamCreateWithFlags(s, f) hu_stream(s)
 #define cudaStreamSynchronize(s) hu_ok()
 #define cudaStreamDestroy(s) hu_ok()

@@ -20,6 +20,8 @@ cudaError_t prepare_step_tiled(size_t) { return cudaSuccess; }
 cudaError_t launch_step_chain(const StepArgs&, int, int, bool, bool, bool, cudaStream_t) { return cudaSuccess; }
 cudaError_t launch_forces_chain(const StepArgs&, int, int, int, cudaStream_t) { return cudaSuccess; }
 cudaError_t prepare_step_chain(size_t) { return cudaSuccess; }
+cudaError_t launch_step_staged(const StepArgs&, int, int, bool, bool, bool, cudaStream_t) { return cudaSuccess; }
+cudaError_t prepare_step_staged(size_t) { return cudaSuccess; }
 cudaError_t launch_drift(const StepArgs&, int, int, bool, cudaStream_t) { return cudaSuccess; }
 cudaError_t launch_forces_only(const StepArgs&, int, int, int, cudaStream_t) { return cudaSuccess; }
 cudaError_t launch_reset_energy(float4*, float4*, float4*, int, cudaStream_t) { return cudaSuccess; }

@@ -308,3 +308,55 @@ def test_autotune_leaves_state_unchanged():
     b.step(20)
     for f in FIELDS:
         np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f)
+
+
+@pytest.mark.parametrize("shape", [(64, 1), (64, 2), (96, 8), (128, 4), (192, 2), (256, 8), (128, 0)])
+def test_staged_kernel_shapes_bit_exact_vs_mirror(oracle_built, shape):
+    """The staged chain kernel at several shapes -- including rounds of fewer
+    contact items than a tile holds, so a bead's contacts straddle rounds --
+    and the unstaged chain kernel give the mirror's bits, statuses included."""
+    m = g.tensile_network(seed=17, fibres=90, beads=40, box=(60.0, 40.0, 8.0), z_range=(1.0, 7.0),
+                          fail_mu=np.log(0.6), fail_sigma=0.4, clamp_lo=2.0, clamp_hi=58.0,
+                          pull=0.5, cell=2.5, min_sep=0.9)
+    o = po.OracleSim(m, po.MODE_MIRROR, cell_cap=64, list_cap=64)
+    s = sim(m, list_capacity=64, use_graphs=True)
+    s.set_kernel_shape(*shape)
+    st = s.stats()
+    assert (st["block_size"], st["items_per_thread"]) == shape
+    for n in (1, 9, 30, 60):
+        s.step(n)
+        o.run(n)
+    for f in FIELDS:
+        np.testing.assert_array_equal(s.get(f), o.get(f), err_msg=f"{shape} {f}")
+    np.testing.assert_array_equal(s.status()[0], o.status()[0])
+    np.testing.assert_array_equal(s.status()[1], o.status()[1])
+    assert s.stats()["stalls"] == 0
+    if shape[1] in (1, 2):
+        # rounds of 64 or 128 items: tiles of 60 beads hold more, so a bead's
+        # contacts straddle rounds
+        cnt, _ = s.lists()
+        per_tile = np.add.reduceat(np.minimum(cnt, 64), np.arange(0, m.n_beads, shape[0] - 4))
+        assert per_tile.max() > shape[1] * shape[0]
+
+
+def test_state_save_restore_repeats_steps():
+    """fn_state_restore puts back what fn_state_save took: the same steps from
+    the restored state give the same bits, and the step count goes back."""
+    m = g.tensile_network(seed=19, fibres=40, beads=30, box=(50.0, 40.0, 8.0), z_range=(1.0, 7.0),
+                          fail_mu=np.log(0.6), fail_sigma=0.4, clamp_lo=2.0, clamp_hi=48.0, pull=0.5,
+                          cell=2.5)
+    s = sim(m, list_capacity=64, use_graphs=True)
+    s.step(7)
+    s.save_state()
+    ms = s.step_timed(25)
+    assert ms > 0.0
+    first = {f: s.get(f) for f in FIELDS}
+    st = s.status()
+    assert s.stats()["steps"] == 32
+    for _ in range(2):
+        s.restore_state()
+        assert s.stats()["steps"] == 7
+        s.step(25)
+        for f in FIELDS:
+            np.testing.assert_array_equal(s.get(f), first[f], err_msg=f)
+        np.testing.assert_array_equal(s.status()[0], st[0])
