@@ -722,6 +722,7 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator; reference ships no models)",
             "config": config_dict(m, args, {"half_list_pairs": r["half_pairs"], "block_size": r["block"],
+                                            "items_per_thread": r["stats"]["items_per_thread"],
                                             "storage": "positions f64, velocities/forces f32",
                                             "timed_region": f"fn_step({args.steps}) from one saved state, "
                                                             f"{r['reps']} repetitions, median"}),

@@ -315,9 +315,9 @@ def test_staged_kernel_shapes_bit_exact_vs_mirror(oracle_built, shape):
     """The staged chain kernel at several shapes -- including rounds of fewer
     contact items than a tile holds, so a bead's contacts straddle rounds --
     and the unstaged chain kernel give the mirror's bits, statuses included."""
-    m = g.tensile_network(seed=17, fibres=90, beads=40, box=(60.0, 40.0, 8.0), z_range=(1.0, 7.0),
-                          fail_mu=np.log(0.6), fail_sigma=0.4, clamp_lo=2.0, clamp_hi=58.0,
-                          pull=0.5, cell=2.5, min_sep=0.9)
+    m = g.tensile_network(seed=17, fibres=90, beads=40, box=(70.0, 50.0, 10.0), z_range=(1.0, 9.0),
+                          fail_mu=np.log(0.6), fail_sigma=0.4, clamp_lo=2.0, clamp_hi=68.0,
+                          pull=0.5, cell=2.5, placement="host")
     o = po.OracleSim(m, po.MODE_MIRROR, cell_cap=64, list_cap=64)
     s = sim(m, list_capacity=64, use_graphs=True)
     s.set_kernel_shape(*shape)
