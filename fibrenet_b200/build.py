@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfibrenet.so")
 CLI = os.path.join(HERE, "fibrenet_run")
-SOURCES = ["fn_kernels.cu", "fn_engine.cu", "fn_adjoint.cu", "fn_generate.cpp", "fn_io.cpp"]
+SOURCES = ["fn_kernels.cu", "fn_engine.cu", "fn_adjoint.cu", "fn_upload.cu", "fn_generate.cpp", "fn_io.cpp"]
 HEADERS = ["fn_kernels.h", "fn_types.h", "fn_detmath.h", "fn_device.cuh", "fn_engine_internal.h",
            "fn_cli.cpp"]
 

@@ -821,6 +821,7 @@ FN_API int fn_adjoint_forward(fn_ctx* c, int nsamples, int every, int checkpoint
     fnh::NvtxRange nvtx_range_("fn_adjoint_forward");
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     if (nsamples <= 0 || every <= 0 || checkpoint_every <= 0 || checkpoint_every % every != 0)
         return fail(c, FN_ERR_ARG, "fn_adjoint_forward: checkpoint_every must be a positive multiple of every");
     if (c->damp) return fail(c, FN_ERR_ARG, "fn_adjoint_forward: damping must be 0 (velocity-dependent forces are not differentiated)");
@@ -886,6 +887,7 @@ FN_API int fn_adjoint_backward(fn_ctx* c, const double* dloss_dreaction, double*
     fnh::NvtxRange nvtx_range_("fn_adjoint_backward");
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     AdjointState* S = c->adj;
     if (!S || S->version != c->state_version)
         return fail(c, FN_ERR_STATE, "fn_adjoint_backward: no forward pass matches the current state");

@@ -36,9 +36,10 @@ using fnh::NetHost;
 
 namespace {
 
-/* contact items per thread and round of the staged chain kernel at upload
-   (fn_autotune may pick another) */
-constexpr int kDefaultItemsPerThread = 4;
+/* contact items per thread and round of the staged chain kernel at upload:
+   0, the unstaged chain kernel, which measured faster on the tensile and
+   dense networks (fn_autotune may pick a staged shape) */
+constexpr int kDefaultItemsPerThread = 0;
 
 /* Largest listing radius squared of one network (kernel.cl:632-650): the
    cutoff for lj/st pairs, largest radius + largest skin for hs pairs. */
@@ -204,6 +205,9 @@ void free_all(fn_ctx* c) {
     dfree(c, c->cell_beads);
     dfree(c, c->ref_img);
     dfree(c, c->inv_d);
+    dfree(c, c->perm_d);
+    dfree(c, c->sp_bead_d);
+    dfree(c, c->an_bead_d);
     dfree(c, c->export_xyz);
     dfree(c, c->gate);
     dfree(c, c->list_count);
@@ -631,7 +635,6 @@ bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<
     if (h2d(c, c->ch_sp, chs) || h2d(c, c->ch_an, cha) || h2d(c, c->ch_flags, fl) ||
         h2d(c, c->ch_status, st))
         return false;
-    c->ch_flags_h = fl;
     return true;
 }
 
@@ -641,6 +644,8 @@ bool build_chain(fn_ctx* c, const std::vector<int2>& sp_ends, const std::vector<
    it at upload. */
 int ensure_incidence(fn_ctx* c) {
     if (c->incidence_ready) return FN_OK;
+    int r0 = ensure_host(c);
+    if (r0) return r0;
     const long long nb = c->nb, ns = c->ns, na = c->na;
     const std::vector<int2>& sp_ends = c->sp_ends_h;
     const std::vector<int4>& an_b = c->an_b_h;
@@ -968,6 +973,36 @@ int check_ready(fn_ctx* c) {
     return FN_OK;
 }
 
+int ensure_host(fn_ctx* c) {
+    if (!c->host_stale) return FN_OK;
+    const size_t nb = (size_t)c->nb, ns = (size_t)c->ns, na = (size_t)c->na;
+    c->perm.resize(nb);
+    c->inv.resize(nb);
+    c->sp_ends_h.resize(ns);
+    c->sp_par_h.resize(ns);
+    c->an_b_h.resize(na);
+    c->an_s_h.resize(na);
+    c->an_par_h.resize(na);
+    c->sp_bead.resize(ns);
+    c->an_bead.resize(na);
+    auto d2h = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream) : cudaSuccess;
+    };
+    CK(cudaSetDevice(c->cfg.device));
+    CK(d2h(c->perm.data(), c->perm_d.p, sizeof(int) * nb));
+    CK(d2h(c->inv.data(), c->inv_d.p, sizeof(int) * nb));
+    CK(d2h(c->sp_ends_h.data(), c->sp_ends.p, sizeof(int2) * ns));
+    CK(d2h(c->sp_par_h.data(), c->sp_par.p, sizeof(float4) * ns));
+    CK(d2h(c->an_b_h.data(), c->an_b.p, sizeof(int4) * na));
+    CK(d2h(c->an_s_h.data(), c->an_s.p, sizeof(int2) * na));
+    CK(d2h(c->an_par_h.data(), c->an_par.p, sizeof(float2) * na));
+    CK(d2h(c->sp_bead.data(), c->sp_bead_d.p, sizeof(int) * ns));
+    CK(d2h(c->an_bead.data(), c->an_bead_d.p, sizeof(int) * na));
+    CK(cudaStreamSynchronize(c->stream));
+    c->host_stale = false;
+    return FN_OK;
+}
+
 }  // namespace fnh
 
 using namespace fnh;
@@ -1020,38 +1055,29 @@ FN_API void fn_destroy(fn_ctx* c) {
 
 FN_API const char* fn_last_error(const fn_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-/* fn_upload's work; fn_upload turns the host's exceptions into status codes. */
-static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
-    fnh::NvtxRange nvtx_range_("fn_upload");
-    if (c) c->state_version++;
-    if (!c || n_networks <= 0 || !nets) return fail(c, FN_ERR_ARG, "fn_upload: bad arguments");
-    CK(cudaSetDevice(c->cfg.device));
-    CK(cudaStreamSynchronize(c->stream));
-    drop_graphs(c);
-    c->uploaded = false;
-    c->snap_valid = false;
-    c->n_nets = n_networks;
-    c->nets_h.assign(n_networks, FnNet{});
-    c->info.assign(n_networks, NetHost{});
-    c->pairs_h.clear();
-    long long nb = 0, ns = 0, na = 0, ncells = 0;
-    c->damp = false;
-    for (int k = 0; k < n_networks; ++k) {
-        const fn_network_desc& d = nets[k];
-        if (d.n_beads <= 0 || d.n_springs < 0 || d.n_angles < 0)
-            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": empty or negative sizes");
-        if (!d.type || !d.tag || !d.loc_id || !d.radius || !d.mass || !d.pos || !d.vel ||
-            !d.vel_old || !d.force || !d.img || !d.pair_kind || !d.pair_raw)
-            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null bead array");
-        if (d.n_springs > 0 && (!d.s_type || !d.s_p1 || !d.s_p2 || !d.s_rest || !d.s_k || !d.s_c1 || !d.s_c2))
-            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null spring array");
-        if (d.n_angles > 0 && (!d.a_type || !d.a_b1 || !d.a_b2 || !d.a_b3 || !d.a_s1 || !d.a_s2 ||
-                               !d.a_theta0 || !d.a_k))
-            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null angle array");
-        int r = derive_net(c, d.settings, c->nets_h[k], k);
-        if (r) return r;
-        FnNet& N = c->nets_h[k];
-        const int nt = d.settings.n_types;
+/* fn_upload's per-network preamble: argument checks, the network's kernel
+   constants and pair table entries, its bead / spring / angle / cell ranges
+   (appended to nb, ns, na, ncells).  With element_checks the index checks of
+   every bead, spring and angle and the radius extremes run here on host
+   threads; the device path leaves both to its kernels and fills the extremes
+   in afterwards (set_radius_extremes). */
+static int net_preamble(fn_ctx* c, int k, const fn_network_desc& d, long long& nb, long long& ns, long long& na,
+                        long long& ncells, bool element_checks) {
+    if (d.n_beads <= 0 || d.n_springs < 0 || d.n_angles < 0)
+        return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": empty or negative sizes");
+    if (!d.type || !d.tag || !d.loc_id || !d.radius || !d.mass || !d.pos || !d.vel ||
+        !d.vel_old || !d.force || !d.img || !d.pair_kind || !d.pair_raw)
+        return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null bead array");
+    if (d.n_springs > 0 && (!d.s_type || !d.s_p1 || !d.s_p2 || !d.s_rest || !d.s_k || !d.s_c1 || !d.s_c2))
+        return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null spring array");
+    if (d.n_angles > 0 && (!d.a_type || !d.a_b1 || !d.a_b2 || !d.a_b3 || !d.a_s1 || !d.a_s2 ||
+                           !d.a_theta0 || !d.a_k))
+        return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": null angle array");
+    int r = derive_net(c, d.settings, c->nets_h[k], k);
+    if (r) return r;
+    FnNet& N = c->nets_h[k];
+    const int nt = d.settings.n_types;
+    if (element_checks) {
         /* the first offending bead, spring or angle, as a sequential sweep
            would report it */
         const int nbk = d.n_beads, nsk = d.n_springs;
@@ -1087,126 +1113,183 @@ static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) 
             return fail(c, FN_ERR_ARG, "network " + std::to_string(k) + ": HR_FL angle " +
                                            std::to_string(bad_angle) + " references a missing spring");
         }
-        const int npairs = nt * (nt + 1) / 2;
-        N.pair_base = (int)c->pairs_h.size();
-        bool any_cut = false, any_hs = false;
-        for (int p = 0; p < npairs; ++p) {
-            FnPair P;
-            pair_coeffs(d.pair_kind[p], d.pair_raw + 4 * p, P);
-            if (P.kind == FN_PAIR_HSR && !(P.c[2] <= d.settings.cutoff))
-                return fail(c, FN_ERR_ARG, "network " + std::to_string(k) +
-                                               ": hsr soft radius exceeds the cutoff (pairs would go unlisted)");
-            c->pairs_h.push_back(P);
-            any_cut |= P.kind == FN_PAIR_LJ || P.kind == FN_PAIR_ST || P.kind == FN_PAIR_HSR;
-            any_hs |= P.kind == FN_PAIR_HS || P.kind == FN_PAIR_HSR;
-        }
-        /* largest listing radius (squared): cutoff for lj/st, the largest
-           radius + the largest skin for hs (kernel.cl:632-650) */
-        double rmax = 0.0, smax = 0.0, gap = 1e300;
-        std::mutex red;
-        parallel_for(d.n_beads, [&](long long i0, long long i1) {
-            double r = 0.0, sm = 0.0, g = 1e300;
-            for (long long i = i0; i < i1; ++i) {
-                const float rad = (float)d.radius[i];
-                const float skin = (float)((double)rad + d.settings.skin_ratio);
-                r = std::max(r, (double)rad);
-                sm = std::max(sm, (double)skin);
-                g = std::min(g, (double)skin - (double)rad);
-            }
-            std::lock_guard<std::mutex> lk(red);
-            rmax = std::max(rmax, r);
-            smax = std::max(smax, sm);
-            gap = std::min(gap, g);
-        });
-        c->info[k].skin_gap = gap;
-        c->info[k].any_cut = any_cut;
-        c->info[k].any_hs = any_hs;
-        c->info[k].rmax = rmax;
-        N.list_r2_max = list_r2(c->info[k], N.list_cut_sq, smax);
-        NetHost& h = c->info[k];
-        h.bead_begin = (int)nb;
-        h.bead_end = (int)(nb + d.n_beads);
-        h.spring_begin = (int)ns;
-        h.spring_end = (int)(ns + d.n_springs);
-        h.angle_begin = (int)na;
-        h.angle_end = (int)(na + d.n_angles);
-        h.cell_begin = ncells;
-        h.cell_end = ncells + (long long)N.nx * N.ny * N.nz;
-        h.grid_update_freq = d.settings.grid_update_freq;
-        h.damping = N.damping;
-        N.cell_base = (int)ncells;
-        N.bead_begin = h.bead_begin;
-        N.bead_end = h.bead_end;
-        if (N.damping != 0.0) c->damp = true;
-        if (h.grid_update_freq <= 0) return fail(c, FN_ERR_ARG, "grid_update_freq must be positive");
-        if (k > 0 && h.grid_update_freq != c->info[0].grid_update_freq)
-            return fail(c, FN_ERR_UNSUPPORTED, "all networks of a batch must share grid_update_freq");
-        nb += d.n_beads;
-        ns += d.n_springs;
-        na += d.n_angles;
-        ncells = h.cell_end;
-        if (nb > 0x7fffffffLL || ns > 0x3fffffffLL || na > 0x1fffffffLL || ncells > 0x7fffffffLL)
-            return fail(c, FN_ERR_ARG, "model too large for 32-bit indices");
     }
+    const int npairs = nt * (nt + 1) / 2;
+    N.pair_base = (int)c->pairs_h.size();
+    bool any_cut = false, any_hs = false;
+    for (int p = 0; p < npairs; ++p) {
+        FnPair P;
+        pair_coeffs(d.pair_kind[p], d.pair_raw + 4 * p, P);
+        if (P.kind == FN_PAIR_HSR && !(P.c[2] <= d.settings.cutoff))
+            return fail(c, FN_ERR_ARG, "network " + std::to_string(k) +
+                                           ": hsr soft radius exceeds the cutoff (pairs would go unlisted)");
+        c->pairs_h.push_back(P);
+        any_cut |= P.kind == FN_PAIR_LJ || P.kind == FN_PAIR_ST || P.kind == FN_PAIR_HSR;
+        any_hs |= P.kind == FN_PAIR_HS || P.kind == FN_PAIR_HSR;
+    }
+    /* largest listing radius (squared): cutoff for lj/st, the largest
+       radius + the largest skin for hs (kernel.cl:632-650) */
+    double rmax = 0.0, smax = 0.0, gap = 1e300;
+    std::mutex red;
+    if (element_checks)
+        parallel_for(d.n_beads, [&](long long i0, long long i1) {
+        double r = 0.0, sm = 0.0, g = 1e300;
+        for (long long i = i0; i < i1; ++i) {
+            const float rad = (float)d.radius[i];
+            const float skin = (float)((double)rad + d.settings.skin_ratio);
+            r = std::max(r, (double)rad);
+            sm = std::max(sm, (double)skin);
+            g = std::min(g, (double)skin - (double)rad);
+        }
+        std::lock_guard<std::mutex> lk(red);
+        rmax = std::max(rmax, r);
+        smax = std::max(smax, sm);
+        gap = std::min(gap, g);
+    });
+    c->info[k].skin_gap = gap;
+    c->info[k].any_cut = any_cut;
+    c->info[k].any_hs = any_hs;
+    c->info[k].rmax = rmax;
+    N.list_r2_max = list_r2(c->info[k], N.list_cut_sq, smax);
+    NetHost& h = c->info[k];
+    h.bead_begin = (int)nb;
+    h.bead_end = (int)(nb + d.n_beads);
+    h.spring_begin = (int)ns;
+    h.spring_end = (int)(ns + d.n_springs);
+    h.angle_begin = (int)na;
+    h.angle_end = (int)(na + d.n_angles);
+    h.cell_begin = ncells;
+    h.cell_end = ncells + (long long)N.nx * N.ny * N.nz;
+    h.grid_update_freq = d.settings.grid_update_freq;
+    h.damping = N.damping;
+    N.cell_base = (int)ncells;
+    N.bead_begin = h.bead_begin;
+    N.bead_end = h.bead_end;
+    if (N.damping != 0.0) c->damp = true;
+    if (h.grid_update_freq <= 0) return fail(c, FN_ERR_ARG, "grid_update_freq must be positive");
+    if (k > 0 && h.grid_update_freq != c->info[0].grid_update_freq)
+        return fail(c, FN_ERR_UNSUPPORTED, "all networks of a batch must share grid_update_freq");
+    nb += d.n_beads;
+    ns += d.n_springs;
+    na += d.n_angles;
+    ncells = h.cell_end;
+    if (nb > 0x7fffffffLL || ns > 0x3fffffffLL || na > 0x1fffffffLL || ncells > 0x7fffffffLL)
+        return fail(c, FN_ERR_ARG, "model too large for 32-bit indices");
+    return FN_OK;
+}
+
+/* largest radius, largest skin radius and smallest skin - radius of network
+   k: the listing radius of its hs pairs and the displacement threshold */
+static void set_radius_extremes(fn_ctx* c, int k, double rmax, double smax, double gap) {
+    c->info[k].skin_gap = gap;
+    c->info[k].rmax = rmax;
+    c->nets_h[k].list_r2_max = list_r2(c->info[k], c->nets_h[k].list_cut_sq, smax);
+}
+
+/* The context's device buffers for a model of these sizes, whichever path
+   converts the model. */
+static cudaError_t alloc_model(fn_ctx* c, long long nb, long long ns, long long na, long long ncells, int n_networks,
+                               std::string& what) {
+    cudaError_t e = cudaSuccess;
+#define AL(call)                   \
+    do {                           \
+        if ((e = (call)) != cudaSuccess) { \
+            what = #call;          \
+            return e;              \
+        }                          \
+    } while (0)
+    const size_t list_n = (size_t)c->list_stride * (size_t)c->cfg.list_capacity;
+    for (int k = 0; k < 2; ++k) {
+        AL(dalloc(c, c->pos[k], nb));
+        AL(dalloc(c, c->img[k], nb));
+    }
+    AL(dalloc(c, c->vold, nb));
+    AL(dalloc(c, c->force, nb));
+    AL(dalloc(c, c->vel, nb));
+    AL(dalloc(c, c->binfo, nb));
+    AL(dalloc(c, c->sp_ends, ns));
+    AL(dalloc(c, c->sp_par, ns));
+    AL(dalloc(c, c->sp_type, ns));
+    AL(dalloc(c, c->sp_status, ns));
+    AL(dalloc(c, c->an_b, na));
+    AL(dalloc(c, c->an_s, na));
+    AL(dalloc(c, c->an_par, na));
+    AL(dalloc(c, c->an_status, na));
+    AL(dalloc(c, c->cell_of, nb));
+    AL(dalloc(c, c->cell_count, ncells));
+    AL(dalloc(c, c->cell_fill, ncells));
+    AL(dalloc(c, c->cell_start, ncells + 1));
+    AL(dalloc(c, c->cell_beads, nb));
+    AL(dalloc(c, c->list_count, nb));
+    AL(dalloc(c, c->list, list_n));
+    AL(dalloc(c, c->scan_sums, (size_t)std::max(fn::scan_block_count(ncells), fn::scan_block_count(nb)) + 1));
+    AL(dalloc(c, c->nets, n_networks));
+    AL(dalloc(c, c->pairs, c->pairs_h.size()));
+    AL(dalloc(c, c->counters, FN_CNT_N));
+    AL(dalloc(c, c->obs_partial, 5 * 1024));
+    AL(dalloc(c, c->obs_out, 8));
+    AL(dalloc(c, c->en_partial, (size_t)fn::FN_EN_N * 1024));
+    AL(dalloc(c, c->en_out, fn::FN_EN_N));
+#undef AL
+    return cudaSuccess;
+}
+
+/* The context's totals once every network's preamble has run. */
+static void set_totals(fn_ctx* c, long long nb, long long ns, long long na, long long ncells) {
     c->nb = nb;
     c->ns = ns;
     c->na = na;
     c->ncells = ncells;
     c->list_stride = (int)((nb + 31) / 32 * 32);
-    /* the export's copy of the numbering is rebuilt on first use; freed
-       here, before the helper thread below starts to allocate (both update
-       the context's device-byte count) */
+    c->grid_update_freq = c->info[0].grid_update_freq;
+}
+
+/* What fn_upload resets before either path runs. */
+static int upload_begin(fn_ctx* c, int n_networks) {
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->uploaded = false;
+    c->snap_valid = false;
+    c->n_nets = n_networks;
+    c->nets_h.assign(n_networks, FnNet{});
+    c->info.assign(n_networks, NetHost{});
+    c->pairs_h.clear();
+    c->damp = false;
+    c->host_stale = false;
+    c->uploaded_on_device = false;
+    c->incidence_ready = false;
+    /* freed before any helper thread allocates (all update the context's
+       device-byte count) */
     dfree(c, c->inv_d);
+    dfree(c, c->perm_d);
+    dfree(c, c->sp_bead_d);
+    dfree(c, c->an_bead_d);
+    return FN_OK;
+}
+
+/* The host path of fn_upload: checks, bead order and conversion on host
+   threads, device allocations and copies overlapped with them.  Runs for
+   every model the device path does not take. */
+static int upload_host(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
+    int r0 = upload_begin(c, n_networks);
+    if (r0) return r0;
+    long long nb = 0, ns = 0, na = 0, ncells = 0;
+    for (int k = 0; k < n_networks; ++k) {
+        int r = net_preamble(c, k, nets[k], nb, ns, na, ncells, true);
+        if (r) return r;
+    }
+    set_totals(c, nb, ns, na, ncells);
     /* device allocations on a helper thread while this one orders and
        converts the model (the sizes are known from here on) */
     cudaError_t alloc_err = cudaSuccess;
     std::string alloc_what;
     std::thread allocator([&, nb, ns, na, ncells, n_networks] {
         if ((alloc_err = cudaSetDevice(c->cfg.device)) != cudaSuccess) return;
-#define AL(call)                          \
-    do {                                  \
-        if ((alloc_err = (call)) != cudaSuccess) { \
-            alloc_what = #call;           \
-            return;                       \
-        }                                 \
-    } while (0)
-    const size_t list_n = (size_t)c->list_stride * (size_t)c->cfg.list_capacity;
-        for (int k = 0; k < 2; ++k) {
-            AL(dalloc(c, c->pos[k], nb));
-            AL(dalloc(c, c->img[k], nb));
-        }
-        AL(dalloc(c, c->vold, nb));
-        AL(dalloc(c, c->force, nb));
-        AL(dalloc(c, c->vel, nb));
-        AL(dalloc(c, c->binfo, nb));
-        AL(dalloc(c, c->sp_ends, ns));
-        AL(dalloc(c, c->sp_par, ns));
-        AL(dalloc(c, c->sp_type, ns));
-        AL(dalloc(c, c->sp_status, ns));
-        AL(dalloc(c, c->an_b, na));
-        AL(dalloc(c, c->an_s, na));
-        AL(dalloc(c, c->an_par, na));
-        AL(dalloc(c, c->an_status, na));
-        AL(dalloc(c, c->cell_of, nb));
-        AL(dalloc(c, c->cell_count, ncells));
-        AL(dalloc(c, c->cell_fill, ncells));
-        AL(dalloc(c, c->cell_start, ncells + 1));
-        AL(dalloc(c, c->cell_beads, nb));
-        AL(dalloc(c, c->list_count, nb));
-        AL(dalloc(c, c->list, list_n));
-        AL(dalloc(c, c->scan_sums, (size_t)fn::scan_block_count(ncells) + 1));
-        AL(dalloc(c, c->nets, n_networks));
-        AL(dalloc(c, c->pairs, c->pairs_h.size()));
-        AL(dalloc(c, c->counters, FN_CNT_N));
-        AL(dalloc(c, c->obs_partial, 5 * 1024));
-        AL(dalloc(c, c->obs_out, 8));
-        AL(dalloc(c, c->en_partial, (size_t)fn::FN_EN_N * 1024));
-        AL(dalloc(c, c->en_out, fn::FN_EN_N));
-#undef AL
+        alloc_err = alloc_model(c, nb, ns, na, ncells, n_networks, alloc_what);
     });
     JoinOnExit join_allocator{allocator};
 
-    c->grid_update_freq = c->info[0].grid_update_freq;
 
     /* bead order */
     c->perm.assign(nb, 0);
@@ -1227,8 +1310,6 @@ static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) 
     HostArray<double4> pos(nb), img(nb);
     HostArray<float4> vold(nb), force(nb), vel(nb);
     HostArray<int4> binfo(nb);
-    c->mass_h.resize(nb);
-    c->radius_h.resize(nb);
     for (int k = 0; k < n_networks; ++k) {
         const fn_network_desc& d = nets[k];
         const int base = c->info[k].bead_begin;
@@ -1238,8 +1319,6 @@ static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) 
             const float rad = (float)d.radius[i];
             const double mass = d.mass[i];
             const double minv = mass > 0.0 ? 1.0 / mass : 0.0; /* SimulationManager.cpp:1435-1445 */
-            c->mass_h[base + i] = mass;
-            c->radius_h[base + i] = d.radius[i];
             pos[q] = make_double4(d.pos[3 * i], d.pos[3 * i + 1], d.pos[3 * i + 2], pack_w(rad, d.type[i]));
             img[q] = make_double4(d.img[3 * i], d.img[3 * i + 1], d.img[3 * i + 2], minv);
             vold[q] = make_float4((float)d.vel_old[3 * i], (float)d.vel_old[3 * i + 1],
@@ -1358,9 +1437,278 @@ static int upload_model(fn_ctx* c, int n_networks, const fn_network_desc* nets) 
     return FN_OK;
 }
 
+/* fn_upload returns this internally when the device path leaves the model to
+   the host path */
+constexpr int kUploadFallback = -1;
+
+/* Stream-ordered scratch of the device path, returned to the pool on every
+   way out. */
+struct StreamScratch {
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    ~StreamScratch() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+
+/* The device path of fn_upload: the caller's arrays are copied to the device
+   as they are (one copy per array and network) and checked, ordered and
+   converted there (fn_upload.cu); the host sorts one key per fibre.  It takes
+   models whose every spring joins consecutive beads (fibres stored bead
+   after bead) and whose bonds are in chain form, and leaves every other
+   model -- and every invalid one, whose error the host path then reports
+   exactly as before -- to the host path (kUploadFallback).  The staged
+   arrays are the host path's, bit for bit. */
+static int upload_device(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
+    int r = upload_begin(c, n_networks);
+    if (r) return r;
+    long long nb = 0, ns = 0, na = 0, ncells = 0;
+    for (int k = 0; k < n_networks; ++k)
+        if (net_preamble(c, k, nets[k], nb, ns, na, ncells, false)) return kUploadFallback;
+    set_totals(c, nb, ns, na, ncells);
+    std::string what;
+    cudaError_t e = alloc_model(c, nb, ns, na, ncells, n_networks, what);
+    if (e != cudaSuccess)
+        return fail(c, e == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA, what + ": " + cudaGetErrorString(e));
+    CK(dalloc(c, c->inv_d, (size_t)nb));
+    CK(dalloc(c, c->export_xyz, (size_t)(3 * nb)));
+    CK(dalloc(c, c->perm_d, (size_t)nb));
+    CK(dalloc(c, c->sp_bead_d, (size_t)ns));
+    CK(dalloc(c, c->an_bead_d, (size_t)na));
+    CK(dalloc(c, c->ch_sp, (size_t)nb));
+    CK(dalloc(c, c->ch_an, (size_t)nb));
+    CK(dalloc(c, c->ch_flags, (size_t)nb));
+    CK(dalloc(c, c->ch_status, (size_t)nb));
+
+    /* one stream-ordered block for the staged caller arrays and the
+       temporaries, carved in 256-byte aligned pieces */
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) / 256 * 256;
+        return o;
+    };
+    const size_t o_type = take(4 * nb), o_tag = take(4 * nb), o_loc = take(4 * nb), o_rad = take(8 * nb),
+                 o_mass = take(8 * nb), o_pos = take(24 * nb), o_vel = take(24 * nb), o_vold = take(24 * nb),
+                 o_frc = take(24 * nb), o_img = take(24 * nb);
+    const size_t o_stype = take(4 * ns), o_p1 = take(4 * ns), o_p2 = take(4 * ns), o_rest = take(8 * ns),
+                 o_sk = take(8 * ns), o_c1 = take(8 * ns), o_c2 = take(8 * ns);
+    const size_t o_atype = take(4 * na), o_b1 = take(4 * na), o_b2 = take(4 * na), o_b3 = take(4 * na),
+                 o_s1 = take(4 * na), o_s2 = take(4 * na), o_th = take(8 * na), o_ak = take(8 * na);
+    const size_t o_nets = take(sizeof(fn::UpNet) * n_networks), o_chk = take(sizeof(fn::UpCheck) * n_networks);
+    const size_t o_link = take(nb), o_flag = take(4 * nb), o_runof = take(4 * (nb + 1)), o_start = take(4 * nb),
+                 o_key = take(8 * nb), o_runout = take(4 * nb), o_next = take(4 * nb), o_centre = take(4 * nb),
+                 o_fl = take(nb), o_fa = take(nb), o_bad = take(4);
+    StreamScratch sc;
+    sc.s = c->stream;
+    CK(cudaMallocAsync(&sc.p, off, c->stream));
+    char* base = static_cast<char*>(sc.p);
+    auto at = [&](size_t o) { return (void*)(base + o); };
+
+    std::vector<fn::UpNet> un(n_networks);
+    std::vector<fn::UpCheck> chk(n_networks);
+    for (int k = 0; k < n_networks; ++k) {
+        const NetHost& h = c->info[k];
+        fn::UpNet& u = un[k];
+        u.bead_begin = h.bead_begin;
+        u.bead_end = h.bead_end;
+        u.spring_begin = h.spring_begin;
+        u.spring_end = h.spring_end;
+        u.angle_begin = h.angle_begin;
+        u.angle_end = h.angle_end;
+        u.n_types = nets[k].settings.n_types;
+        u.pad_ = 0;
+        for (int a = 0; a < 3; ++a) u.box[a] = nets[k].settings.box[a];
+        u.skin_ratio = nets[k].settings.skin_ratio;
+        chk[k].bad_bead = chk[k].bad_spring = chk[k].bad_angle = 0x7fffffff;
+        chk[k].not_runs = 0;
+        chk[k].rmax = chk[k].smax = 0ull;
+        chk[k].gmin = ~0ull;
+    }
+    /* the caller's arrays, network by network */
+    for (int k = 0; k < n_networks; ++k) {
+        const fn_network_desc& d = nets[k];
+        const NetHost& h = c->info[k];
+        const size_t b = (size_t)h.bead_begin, n = (size_t)d.n_beads;
+        const size_t sb = (size_t)h.spring_begin, sn = (size_t)d.n_springs;
+        const size_t ab = (size_t)h.angle_begin, an = (size_t)d.n_angles;
+        auto cp = [&](size_t o, size_t first, size_t count, size_t elem, const void* src) -> cudaError_t {
+            if (!count) return cudaSuccess;
+            return cudaMemcpyAsync(base + o + first * elem, src, count * elem, cudaMemcpyHostToDevice, c->stream);
+        };
+        CK(cp(o_type, b, n, 4, d.type));
+        CK(cp(o_tag, b, n, 4, d.tag));
+        CK(cp(o_loc, b, n, 4, d.loc_id));
+        CK(cp(o_rad, b, n, 8, d.radius));
+        CK(cp(o_mass, b, n, 8, d.mass));
+        CK(cp(o_pos, b, n, 24, d.pos));
+        CK(cp(o_vel, b, n, 24, d.vel));
+        CK(cp(o_vold, b, n, 24, d.vel_old));
+        CK(cp(o_frc, b, n, 24, d.force));
+        CK(cp(o_img, b, n, 24, d.img));
+        CK(cp(o_stype, sb, sn, 4, d.s_type));
+        CK(cp(o_p1, sb, sn, 4, d.s_p1));
+        CK(cp(o_p2, sb, sn, 4, d.s_p2));
+        CK(cp(o_rest, sb, sn, 8, d.s_rest));
+        CK(cp(o_sk, sb, sn, 8, d.s_k));
+        CK(cp(o_c1, sb, sn, 8, d.s_c1));
+        CK(cp(o_c2, sb, sn, 8, d.s_c2));
+        CK(cp(o_atype, ab, an, 4, d.a_type));
+        CK(cp(o_b1, ab, an, 4, d.a_b1));
+        CK(cp(o_b2, ab, an, 4, d.a_b2));
+        CK(cp(o_b3, ab, an, 4, d.a_b3));
+        CK(cp(o_s1, ab, an, 4, d.a_s1));
+        CK(cp(o_s2, ab, an, 4, d.a_s2));
+        CK(cp(o_th, ab, an, 8, d.a_theta0));
+        CK(cp(o_ak, ab, an, 8, d.a_k));
+    }
+    CK(cudaMemcpyAsync(at(o_nets), un.data(), sizeof(fn::UpNet) * n_networks, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(at(o_chk), chk.data(), sizeof(fn::UpCheck) * n_networks, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(at(o_link), 0, (size_t)nb, c->stream));
+    fn::UpRaw R;
+    R.type = (const int*)at(o_type);
+    R.tag = (const int*)at(o_tag);
+    R.loc_id = (const int*)at(o_loc);
+    R.radius = (const double*)at(o_rad);
+    R.mass = (const double*)at(o_mass);
+    R.pos = (const double*)at(o_pos);
+    R.vel = (const double*)at(o_vel);
+    R.vel_old = (const double*)at(o_vold);
+    R.force = (const double*)at(o_frc);
+    R.img = (const double*)at(o_img);
+    R.s_type = (const int*)at(o_stype);
+    R.s_p1 = (const int*)at(o_p1);
+    R.s_p2 = (const int*)at(o_p2);
+    R.s_rest = (const double*)at(o_rest);
+    R.s_k = (const double*)at(o_sk);
+    R.s_c1 = (const double*)at(o_c1);
+    R.s_c2 = (const double*)at(o_c2);
+    R.a_type = (const int*)at(o_atype);
+    R.a_b1 = (const int*)at(o_b1);
+    R.a_b2 = (const int*)at(o_b2);
+    R.a_b3 = (const int*)at(o_b3);
+    R.a_s1 = (const int*)at(o_s1);
+    R.a_s2 = (const int*)at(o_s2);
+    R.a_theta0 = (const double*)at(o_th);
+    R.a_k = (const double*)at(o_ak);
+    const fn::UpNet* unets = (const fn::UpNet*)at(o_nets);
+    unsigned char* link = (unsigned char*)at(o_link);
+    int* flag = (int*)at(o_flag);
+    int* run_of = (int*)at(o_runof);
+    int* start = (int*)at(o_start);
+    unsigned long long* key = (unsigned long long*)at(o_key);
+    int* run_out = (int*)at(o_runout);
+
+    /* checks: any offending index, or a spring between non-consecutive
+       beads, leaves the model to the host path */
+    CK(fn::launch_upload_checks(unets, n_networks, R, (fn::UpCheck*)at(o_chk), (int)nb, (int)ns, (int)na, link,
+                                c->stream));
+    const bool reorder = c->cfg.reorder != 0;
+    if (reorder)
+        CK(fn::launch_upload_runs(unets, n_networks, R, link, flag, run_of, c->scan_sums.p, start, key, (int)nb,
+                                  c->stream));
+    int n_runs = 0;
+    CK(cudaMemcpyAsync(chk.data(), at(o_chk), sizeof(fn::UpCheck) * n_networks, cudaMemcpyDeviceToHost, c->stream));
+    if (reorder) CK(cudaMemcpyAsync(&n_runs, run_of + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    auto undkey = [](unsigned long long k) {
+        const unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+        double x;
+        std::memcpy(&x, &u, 8);
+        return x;
+    };
+    for (int k = 0; k < n_networks; ++k) {
+        const fn::UpCheck& q = chk[k];
+        if (q.bad_bead != 0x7fffffff || q.bad_spring != 0x7fffffff || q.bad_angle != 0x7fffffff || q.not_runs)
+            return kUploadFallback;
+        set_radius_extremes(c, k, undkey(q.rmax), undkey(q.smax), undkey(q.gmin));
+    }
+
+    /* bead order: the runs (fibres) of each network sorted by key, as the
+       host path sorts them, and laid out one after the other */
+    if (reorder) {
+        std::vector<int> st(n_runs);
+        std::vector<unsigned long long> ky(n_runs);
+        CK(cudaMemcpyAsync(st.data(), start, sizeof(int) * (size_t)n_runs, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(ky.data(), key, sizeof(unsigned long long) * (size_t)n_runs, cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        std::vector<int> out(n_runs);
+        int r0 = 0;
+        for (int k = 0; k < n_networks; ++k) {
+            const int bb = c->info[k].bead_begin, be = c->info[k].bead_end;
+            int r1 = r0;
+            while (r1 < n_runs && st[r1] < be) ++r1;
+            std::vector<unsigned long long> sorted(ky.begin() + r0, ky.begin() + r1);
+            std::sort(sorted.begin(), sorted.end());
+            int acc = bb;
+            for (unsigned long long kk : sorted) {
+                const int first = bb + (int)(uint32_t)kk;
+                const int rr = (int)(std::lower_bound(st.begin() + r0, st.begin() + r1, first) - st.begin());
+                const int len = (rr + 1 < r1 ? st[rr + 1] : be) - first;
+                out[rr] = acc;
+                acc += len;
+            }
+            r0 = r1;
+        }
+        CK(cudaMemcpyAsync(run_out, out.data(), sizeof(int) * (size_t)n_runs, cudaMemcpyHostToDevice, c->stream));
+    }
+    c->cur = 0;
+    CK(fn::launch_upload_convert(unets, n_networks, R, flag, run_of, start, run_out, reorder ? 1 : 0, c->inv_d.p,
+                                 c->perm_d.p, c->pos[0].p, c->img[0].p, c->vold.p, c->force.p, c->vel.p, c->binfo.p,
+                                 c->sp_ends.p, c->sp_par.p, c->sp_type.p, c->sp_status.p, c->an_b.p, c->an_s.p,
+                                 c->an_par.p, c->an_status.p, (int)nb, (int)ns, (int)na, c->stream));
+    /* chain form: per-bead records, or back to the host path */
+    CK(cudaMemsetAsync(at(o_next), 0xff, 4 * (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(at(o_centre), 0xff, 4 * (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(at(o_fl), 0, (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(at(o_fa), 0, (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(at(o_bad), 0, 4, c->stream));
+    CK(fn::launch_upload_chain(c->sp_ends.p, c->sp_type.p, c->sp_par.p, c->an_b.p, c->an_s.p, c->an_par.p,
+                               (int*)at(o_next), (int*)at(o_centre), (unsigned char*)at(o_fl),
+                               (unsigned char*)at(o_fa), c->ch_sp.p, c->ch_an.p, c->ch_flags.p, c->ch_status.p,
+                               c->sp_bead_d.p, c->an_bead_d.p, (int*)at(o_bad), (int)nb, (int)ns, (int)na,
+                               c->stream));
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, at(o_bad), sizeof bad, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (bad) return kUploadFallback;
+
+    CK(cudaMemcpyAsync(c->pos[1].p, c->pos[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->img[1].p, c->img[0].p, sizeof(double4) * nb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(h2d(c, c->nets, c->nets_h));
+    CK(h2d(c, c->pairs, c->pairs_h));
+    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * FN_CNT_N, c->stream));
+    CK(cudaMemsetAsync(c->list_count.p, 0, sizeof(int) * (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(c->cell_of.p, 0xff, sizeof(int) * (size_t)nb, c->stream));
+    CK(cudaMemsetAsync(c->cell_count.p, 0, sizeof(int) * (size_t)ncells, c->stream));
+    c->chain = true;
+    c->host_stale = true; /* host copies of the numbering and the bonds: on first need */
+    c->uploaded_on_device = true;
+    r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128, c->cfg.chain_mode == 0 ? kDefaultItemsPerThread : 0);
+    if (r) return r;
+    r = verlet_setup(c);
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    c->steps_done = 0;
+    c->rebuilds_done = 0;
+    c->uploaded = true;
+    return FN_OK;
+}
+
+/* fn_upload: the device path when the model is in its reach, else (and
+   for every invalid model, whose error the host path reports) the host path.
+   Host exceptions become status codes. */
 FN_API int fn_upload(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     try {
-        return upload_model(c, n_networks, nets);
+        fnh::NvtxRange nvtx_range_("fn_upload");
+        if (c) c->state_version++;
+        if (!c || n_networks <= 0 || !nets) return fail(c, FN_ERR_ARG, "fn_upload: bad arguments");
+        if (c->cfg.chain_mode != 2 && !c->cfg.host_upload) {
+            const int r = upload_device(c, n_networks, nets);
+            if (r != kUploadFallback) return r;
+        }
+        return upload_host(c, n_networks, nets);
     } catch (const std::bad_alloc&) {
         return fail(c, FN_ERR_OOM, "fn_upload: out of host memory");
     } catch (const std::system_error& e) {
@@ -1497,6 +1845,7 @@ FN_API int fn_set_beads(fn_ctx* c, int field, const double* host) {
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     if (!host) return fail(c, FN_ERR_ARG, "fn_set_beads: null host pointer");
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
@@ -1538,6 +1887,7 @@ FN_API int fn_set_mass(fn_ctx* c, const double* mass) {
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     if (!mass) return fail(c, FN_ERR_ARG, "fn_set_mass: null pointer");
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
@@ -1549,7 +1899,6 @@ FN_API int fn_set_mass(fn_ctx* c, const double* mass) {
     for (long long q = 0; q < nb; ++q) {
         const double m = mass[c->perm[q]];
         tmp[q].w = m > 0.0 ? 1.0 / m : 0.0;
-        c->mass_h[c->perm[q]] = m;
     }
     CK(cudaMemcpy(c->img[c->cur].p, tmp.data(), sizeof(double4) * nb, cudaMemcpyHostToDevice));
     return FN_OK;
@@ -1561,6 +1910,7 @@ FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     if (!skin) return fail(c, FN_ERR_ARG, "fn_set_skin: null pointer");
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
@@ -1569,12 +1919,22 @@ FN_API int fn_set_skin(fn_ctx* c, const double* skin) {
     CK(cudaMemcpy(tmp.data(), c->binfo.p, sizeof(int4) * nb, cudaMemcpyDeviceToHost));
     for (long long q = 0; q < nb; ++q) tmp[q].w = float_bits((float)skin[c->perm[q]]);
     CK(cudaMemcpy(c->binfo.p, tmp.data(), sizeof(int4) * nb, cudaMemcpyHostToDevice));
+    /* radii as stored (float, packed in the position's fourth word), upload order */
+    std::vector<double4> p4(nb);
+    CK(cudaMemcpy(p4.data(), c->pos[c->cur].p, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
+    std::vector<float> radius(nb);
+    for (long long q = 0; q < nb; ++q) {
+        uint64_t bits;
+        std::memcpy(&bits, &p4[q].w, 8);
+        const uint32_t lo = (uint32_t)bits;
+        std::memcpy(&radius[c->perm[q]], &lo, 4);
+    }
     for (int k = 0; k < c->n_nets; ++k) {
         double smax = 0.0;
         double gap = 1e300;
         for (int i = c->info[k].bead_begin; i < c->info[k].bead_end; ++i) {
             smax = std::max(smax, (double)(float)skin[i]);
-            gap = std::min(gap, (double)(float)skin[i] - (double)(float)c->radius_h[i]);
+            gap = std::min(gap, (double)(float)skin[i] - (double)radius[i]);
         }
         c->info[k].skin_gap = gap;
         c->nets_h[k].list_r2_max = list_r2(c->info[k], c->nets_h[k].list_cut_sq, smax);
@@ -1592,6 +1952,7 @@ FN_API int fn_set_springs(fn_ctx* c, const double* rest, const double* k, const 
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
     for (long long s = 0; s < c->ns; ++s) {
@@ -1617,6 +1978,7 @@ FN_API int fn_set_angles(fn_ctx* c, const double* theta0, const double* k) {
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
     for (long long a = 0; a < c->na; ++a) {
@@ -1638,6 +2000,7 @@ FN_API int fn_download_status(fn_ctx* c, int* spring_status, int* angle_status) 
     FN_TRY
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     CK(cudaSetDevice(c->cfg.device));
     if (c->chain) {
         std::vector<unsigned char> st(c->nb);
@@ -1668,6 +2031,7 @@ FN_API int fn_set_status(fn_ctx* c, const int* spring_status, const int* angle_s
     if (c) c->state_version++;
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
     if (c->chain) {
@@ -1862,6 +2226,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     std::memset(out, 0, sizeof *out);
     out->block_size = c->block;
     out->items_per_thread = c->staged ? c->chunk / c->block : 0;
+    out->upload_on_device = c->uploaded_on_device ? 1 : 0;
     out->bond_path = c->chain ? 2 : (c->tiled ? 1 : 0);
     out->graph_launches = c->graph_launches;
     out->n_networks = c->n_nets;
@@ -1890,6 +2255,7 @@ FN_API int fn_get_cells(fn_ctx* c, int* bead_cell, int* cell_count, long long n_
     FN_TRY
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     CK(cudaSetDevice(c->cfg.device));
     if (bead_cell) {
         std::vector<int> tmp(c->nb);
@@ -1910,6 +2276,7 @@ FN_API int fn_get_lists(fn_ctx* c, int* count, int* partners, int cap) {
     FN_TRY
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     CK(cudaSetDevice(c->cfg.device));
     const long long nb = c->nb;
     std::vector<int> cnt(nb);
@@ -1937,6 +2304,7 @@ FN_API int fn_get_permutation(fn_ctx* c, int* perm) {
     FN_TRY
     int r = check_ready(c);
     if (r) return r;
+    if ((r = ensure_host(c))) return r;
     if (!perm) return FN_ERR_ARG;
     std::memcpy(perm, c->perm.data(), sizeof(int) * c->nb);
     return FN_OK;

@@ -64,7 +64,6 @@ struct fn_ctx {
     long long nb = 0, ns = 0, na = 0, ncells = 0;
     std::vector<int> perm;  // internal -> upload
     std::vector<int> inv;   // upload -> internal
-    std::vector<double> mass_h, radius_h;
     std::vector<float4> sp_par_h;  // upload order (springs are not renumbered)
     std::vector<float2> an_par_h;
     bool damp = false;
@@ -95,7 +94,6 @@ struct fn_ctx {
     /* chain form */
     bool chain = false;
     std::vector<int> sp_bead, an_bead; /* spring -> lower bead, angle -> centre bead */
-    std::vector<unsigned char> ch_flags_h;
     DevBuf<float4> ch_sp;
     DevBuf<float2> ch_an;
     DevBuf<unsigned char> ch_flags, ch_status;
@@ -132,6 +130,13 @@ struct fn_ctx {
 
     /* export: upload -> internal bead index on the device, x/y/z staging */
     DevBuf<int> inv_d;
+    /* after the device path of fn_upload: the numbering and the bond arrays
+       exist on the device only, and the host copies above (perm, inv,
+       sp_ends_h, sp_par_h, an_b_h, an_s_h, an_par_h, sp_bead, an_bead) are
+       filled from these on first need (ensure_host) */
+    bool host_stale = false;
+    bool uploaded_on_device = false;
+    DevBuf<int> perm_d, sp_bead_d, an_bead_d;
     DevBuf<double> export_xyz;
 
     /* displacement-triggered rebuilds (cfg.verlet_skin > 0) */
@@ -220,6 +225,9 @@ void dfree(fn_ctx* c, DevBuf<T>& b) {
 }
 
 int check_ready(fn_ctx* c);
+/* fills the host copies of the numbering and the bonds when only the device
+   holds them (after the device path of fn_upload) */
+int ensure_host(fn_ctx* c);
 int ensure_incidence(fn_ctx* c);
 fn::StepArgs step_args(fn_ctx* c, bool pingpong);
 /* one step launch of the kernel the context uses (chain: staged or plain;

@@ -775,7 +775,7 @@ static int run_input(const char* input_path, int device, int strict, char* err, 
     fn_input* in = nullptr;
     int rc = fn_input_read(input_path, strict, &in, err, err_len);
     if (rc) return rc;
-    fn_config cfg = {device, 64, 128, 1, 0, 0, 0};
+    fn_config cfg = {device, 64, 128, 1, 0, 0, 0, 0.0, 0};
     fn_ctx* ctx = nullptr;
     auto finish = [&](int code, const std::string& msg) {
         if (!msg.empty()) copy_err(msg, err, err_len);

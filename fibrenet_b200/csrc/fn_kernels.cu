@@ -1802,6 +1802,15 @@ cudaError_t launch_reset_energy(float4* force, float4* vel, float4* vold, int n,
 
 long long scan_block_count(long long n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
 
+cudaError_t launch_exclusive_scan(const int* in, long long n, int* out, int* block_sums, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const long long nblk = scan_block_count(n);
+    k_scan_partials<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(in, n, block_sums, nullptr);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(block_sums, (int)nblk, out + n, nullptr);
+    k_scan_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(in, n, block_sums, out, nullptr);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, long long ncells,
                            int* scan_block_sums, cudaStream_t s) {
     cudaError_t e;

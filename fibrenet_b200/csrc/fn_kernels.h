@@ -256,6 +256,51 @@ struct EnergyArgs {
     double* partial; /* FN_EN_N doubles per block */
 };
 
+/* device-side upload (fn_upload.cu): per network ranges and settings, the
+   caller's arrays as staged on the device (networks concatenated, model-file
+   order), and the results of the checks */
+struct UpNet {
+    int bead_begin, bead_end, spring_begin, spring_end, angle_begin, angle_end;
+    int n_types, pad_;
+    double box[3];
+    double skin_ratio;
+};
+
+struct UpRaw {
+    const int *type, *tag, *loc_id;
+    const double *radius, *mass, *pos, *vel, *vel_old, *force, *img;
+    const int *s_type, *s_p1, *s_p2;
+    const double *s_rest, *s_k, *s_c1, *s_c2;
+    const int *a_type, *a_b1, *a_b2, *a_b3, *a_s1, *a_s2;
+    const double *a_theta0, *a_k;
+};
+
+struct UpCheck {
+    int bad_bead, bad_spring, bad_angle; /* first offending index, INT_MAX if none */
+    int not_runs;                        /* springs not joining consecutive beads */
+    unsigned long long rmax, smax, gmin; /* order-preserving keys of the radius extremes */
+};
+
+cudaError_t launch_upload_checks(const UpNet* nets, int n_nets, const UpRaw& R, UpCheck* out, int nb, int ns, int na,
+                                 unsigned char* link, cudaStream_t s);
+cudaError_t launch_upload_runs(const UpNet* nets, int n_nets, const UpRaw& R, const unsigned char* link, int* flag,
+                               int* run_of, int* scan_sums, int* start, unsigned long long* key, int nb,
+                               cudaStream_t s);
+cudaError_t launch_upload_convert(const UpNet* nets, int n_nets, const UpRaw& R, const int* flag, const int* run_of,
+                                  const int* start, const int* run_out, int reorder, int* inv, int* perm,
+                                  double4* pos, double4* img, float4* vold, float4* force, float4* vel, int4* binfo,
+                                  int2* sp_ends, float4* sp_par, signed char* sp_type, signed char* sp_status,
+                                  int4* an_b, int2* an_s, float2* an_par, signed char* an_status, int nb, int ns,
+                                  int na, cudaStream_t s);
+cudaError_t launch_upload_chain(const int2* sp_ends, const signed char* sp_type, const float4* sp_par,
+                                const int4* an_b, const int2* an_s, const float2* an_par, int* next_sp,
+                                int* centre_an, unsigned char* fl, unsigned char* fa, float4* chs, float2* cha,
+                                unsigned char* flags, unsigned char* status, int* sp_bead, int* an_bead, int* bad,
+                                int nb, int ns, int na, cudaStream_t s);
+/* exclusive prefix sum of n ints into out[0..n], out[n] the total;
+   block_sums holds scan_block_count(n) + 1 ints */
+cudaError_t launch_exclusive_scan(const int* in, long long n, int* out, int* block_sums, cudaStream_t s);
+
 cudaError_t launch_energy(const EnergyArgs& E, int nblocks, double* out, cudaStream_t s);
 /* one bead field in upload order as x, y, z doubles (inv: upload -> internal) */
 cudaError_t launch_export_xyz(const double4* src, const int* inv, int n, double* out, cudaStream_t s);

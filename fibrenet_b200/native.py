@@ -47,7 +47,7 @@ class FnNetworkDesc(C.Structure):
 class FnConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("cell_capacity", C.c_int), ("list_capacity", C.c_int),
                 ("reorder", C.c_int), ("use_graphs", C.c_int), ("block_size", C.c_int),
-                ("chain_mode", C.c_int), ("verlet_skin", C.c_double)]
+                ("chain_mode", C.c_int), ("verlet_skin", C.c_double), ("host_upload", C.c_int)]
 
 
 class FnStats(C.Structure):
@@ -56,7 +56,7 @@ class FnStats(C.Structure):
                 ("bond_path", C.c_int), ("n_networks", C.c_int), ("n_beads", C.c_longlong),
                 ("device_bytes", C.c_longlong), ("graph_launches", C.c_longlong),
                 ("nonfinite", C.c_longlong), ("items_per_thread", C.c_int),
-                ("stalls", C.c_longlong)]
+                ("stalls", C.c_longlong), ("upload_on_device", C.c_int)]
 
 
 class FnView(C.Structure):
@@ -209,12 +209,13 @@ class Simulation:
 
     def __init__(self, models, device: int = 0, cell_capacity: int = 64, list_capacity: int = 64,
                  reorder: bool = True, use_graphs: bool = False, block_size: int = 0,
-                 chain: bool = True, verlet_skin: float = 0.0, staged: bool = True):
+                 chain: bool = True, verlet_skin: float = 0.0, staged: bool = True,
+                 host_upload: bool = False):
         self.lib = load()
         self.models = [models] if isinstance(models, Model) else list(models)
         chain_mode = (0 if staged else 1) if chain else 2
         cfg = FnConfig(device, cell_capacity, list_capacity, int(reorder), int(use_graphs),
-                       block_size, chain_mode, float(verlet_skin))
+                       block_size, chain_mode, float(verlet_skin), int(host_upload))
         h = C.c_void_p()
         rc = self.lib.fn_create(C.byref(cfg), C.byref(h))
         if rc != FN_OK:

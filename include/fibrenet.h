@@ -131,6 +131,11 @@ typedef struct fn_config {
                            acting radius) since the last rebuild, checked on
                            the device before every step: no pair within reach
                            is ever missed.  Not a reference mode. */
+    int host_upload;    /* 0: fn_upload checks, orders and converts the model
+                           on the device when it can (fibres stored bead
+                           after bead, bonds in chain form), else on host
+                           threads; 1: always on host threads.  Both give the
+                           same device state bit for bit. */
 } fn_config;
 
 /* Counters read back from the device. */
@@ -150,6 +155,8 @@ typedef struct fn_stats {
                                   and round (0: another step kernel) */
     long long stalls;          /* tiles skipped because a bounded wait for their
                                   staged data ran out (fn_sync then fails) */
+    int upload_on_device;      /* 1: the last fn_upload checked, ordered and
+                                  converted the model on the device */
 } fn_stats;
 
 /* A device array of the context, for zero-copy readers (torch through

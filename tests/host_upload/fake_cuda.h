@@ -59,6 +59,8 @@ static inline cudaError_t hu_stream(cudaStream_t* s) {
 #define cudaEventDestroy(e) hu_ok()
 #define cudaMalloc(p, n) hu_malloc((void**)(p), n)
 #define cudaFree(p) hu_free((void*)(p))
+#define cudaMallocAsync(p, n, st) hu_malloc((void**)(p), n)
+#define cudaFreeAsync(p, st) hu_free((void*)(p))
 #define cudaMemcpyAsync(d, s, n, k, st) hu_copy(d, s, n)
 #define cudaMemcpy(d, s, n, k) hu_copy(d, s, n)
 #define cudaMemsetAsync(d, v, n, st) hu_set(d, v, n)

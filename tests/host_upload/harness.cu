@@ -28,6 +28,27 @@ cudaError_t launch_reset_energy(float4*, float4*, float4*, int, cudaStream_t) { 
 long long scan_block_count(long long n) { return (n + 2047) / 2048; }
 cudaError_t launch_rebuild(const RebuildArgs&, int, int, int, long long, int*, cudaStream_t) { return cudaSuccess; }
 cudaError_t launch_observe(const ObserveArgs&, int, double*, cudaStream_t) { return cudaSuccess; }
+/* the device path of fn_upload is never taken here (host_upload = 1) */
+cudaError_t launch_upload_checks(const UpNet*, int, const UpRaw&, UpCheck*, int, int, int, unsigned char*,
+                                 cudaStream_t) {
+    return cudaErrorNotSupported;
+}
+cudaError_t launch_upload_runs(const UpNet*, int, const UpRaw&, const unsigned char*, int*, int*, int*, int*,
+                               unsigned long long*, int, cudaStream_t) {
+    return cudaErrorNotSupported;
+}
+cudaError_t launch_upload_convert(const UpNet*, int, const UpRaw&, const int*, const int*, const int*, const int*,
+                                  int, int*, int*, double4*, double4*, float4*, float4*, float4*, int4*, int2*,
+                                  float4*, signed char*, signed char*, int4*, int2*, float2*, signed char*, int, int,
+                                  int, cudaStream_t) {
+    return cudaErrorNotSupported;
+}
+cudaError_t launch_upload_chain(const int2*, const signed char*, const float4*, const int4*, const int2*,
+                                const float2*, int*, int*, unsigned char*, unsigned char*, float4*, float2*,
+                                unsigned char*, unsigned char*, int*, int*, int*, int, int, int, cudaStream_t) {
+    return cudaErrorNotSupported;
+}
+cudaError_t launch_exclusive_scan(const int*, long long, int*, int*, cudaStream_t) { return cudaErrorNotSupported; }
 cudaError_t launch_verlet_rebuild(const RebuildArgs&, const FnTile*, const double4*, double4*, double, int*, int,
                                   int, int, long long, int*, cudaStream_t) {
     return cudaSuccess;
@@ -42,7 +63,7 @@ void adjoint_free(fn_ctx*) {}
 #define HU_API extern "C" __attribute__((visibility("default")))
 
 HU_API int hu_create(int reorder, int chain_mode, fn_ctx** out) {
-    fn_config cfg = {0, 64, 64, reorder, 0, 128, chain_mode, 0.0};
+    fn_config cfg = {0, 64, 64, reorder, 0, 128, chain_mode, 0.0, 1}; /* the host path under test */
     return fn_create(&cfg, out);
 }
 HU_API int hu_upload(fn_ctx* c, int n, const fn_network_desc* d) { return fn_upload(c, n, d); }
