@@ -64,6 +64,29 @@ uint32_t spread10(uint32_t v) {
 
 namespace fnh {
 
+cudaError_t device_pool(int device, cudaMemPool_t* pool) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess) return e;
+        unsigned long long keep = ~0ull; /* freed memory stays in the pool */
+        e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+        pools[device] = p;
+    }
+    *pool = pools[device];
+    return cudaSuccess;
+}
+
 int fail(fn_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
@@ -213,6 +236,7 @@ void free_all(fn_ctx* c) {
     dfree(c, c->list_count);
     dfree(c, c->list);
     dfree(c, c->scan_sums);
+    dfree(c, c->bricks);
     dfree(c, c->tiles);
     dfree(c, c->nets);
     dfree(c, c->pairs);
@@ -694,6 +718,22 @@ int ensure_incidence(fn_ctx* c) {
     return FN_OK;
 }
 
+/* Bricks of the staged list build: every network's grid cut into bricks of
+   kBrickX x kBrickY x kBrickZ cells (clipped at the grid's far sides). */
+int build_bricks(fn_ctx* c) {
+    std::vector<int4> b;
+    for (int k = 0; k < c->n_nets; ++k) {
+        const FnNet& N = c->nets_h[k];
+        for (int z = 0; z < N.nz; z += fn::kBrickZ)
+            for (int y = 0; y < N.ny; y += fn::kBrickY)
+                for (int x = 0; x < N.nx; x += fn::kBrickX) b.push_back(make_int4(k, x, y, z));
+    }
+    CK(dalloc(c, c->bricks, b.size()));
+    CK(h2d(c, c->bricks, b));
+    c->nbricks = (int)b.size();
+    return FN_OK;
+}
+
 /* Block size (and, for the staged chain kernel, contact items per thread and
    round) of the step kernel: tiles, per-tile tables and kernel attributes.
    items_per_thread 0 selects the plain chain kernel. */
@@ -830,6 +870,8 @@ fn::RebuildArgs rebuild_args(fn_ctx* c) {
     R.cell_cap = c->cfg.cell_capacity;
     R.counters = c->counters.p;
     R.n_nets = c->n_nets;
+    R.bricks = c->list_bricks ? c->bricks.p : nullptr;
+    R.nbricks = c->nbricks;
     R.csr = c->staged ? c->csr.p : nullptr;
     R.csr_region = c->csr_region;
     R.tile_items = c->tile_items.p;
@@ -961,8 +1003,9 @@ int verlet_setup(fn_ctx* c) {
     c->verlet_thresh2 = thresh * thresh;
     if (!c->ref_img.p || c->ref_img.n < (size_t)c->nb) CK(dalloc(c, c->ref_img, (size_t)c->nb));
     if (!c->gate.p) CK(dalloc(c, c->gate, 1));
-    const int one = 1;
-    CK(cudaMemcpy(c->gate.p, &one, sizeof one, cudaMemcpyHostToDevice));
+    static const int one = 1;
+    CK(cudaMemcpyAsync(c->gate.p, &one, sizeof one, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     c->verlet = true;
     return FN_OK;
 }
@@ -1048,6 +1091,7 @@ FN_API void fn_destroy(fn_ctx* c) {
     cudaSetDevice(c->cfg.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_all(c);
+    if (c->stream) cudaStreamSynchronize(c->stream); /* the buffers are back in the pool */
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1425,8 +1469,10 @@ static int upload_host(fn_ctx* c, int n_networks, const fn_network_desc* nets) {
     for (int k = 0; k < 2; ++k)
         if (copy_err[k] != cudaSuccess)
             return fail(c, FN_ERR_CUDA, copy_what[k] + ": " + cudaGetErrorString(copy_err[k]));
-    int r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128,
-                      c->cfg.chain_mode == 0 ? kDefaultItemsPerThread : 0);
+    int r = build_bricks(c);
+    if (r) return r;
+    r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128,
+                  c->cfg.chain_mode == 0 ? kDefaultItemsPerThread : 0);
     if (r) return r;
     r = verlet_setup(c);
     if (r) return r;
@@ -1466,19 +1512,6 @@ static int upload_device(fn_ctx* c, int n_networks, const fn_network_desc* nets)
     for (int k = 0; k < n_networks; ++k)
         if (net_preamble(c, k, nets[k], nb, ns, na, ncells, false)) return kUploadFallback;
     set_totals(c, nb, ns, na, ncells);
-    std::string what;
-    cudaError_t e = alloc_model(c, nb, ns, na, ncells, n_networks, what);
-    if (e != cudaSuccess)
-        return fail(c, e == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA, what + ": " + cudaGetErrorString(e));
-    CK(dalloc(c, c->inv_d, (size_t)nb));
-    CK(dalloc(c, c->export_xyz, (size_t)(3 * nb)));
-    CK(dalloc(c, c->perm_d, (size_t)nb));
-    CK(dalloc(c, c->sp_bead_d, (size_t)ns));
-    CK(dalloc(c, c->an_bead_d, (size_t)na));
-    CK(dalloc(c, c->ch_sp, (size_t)nb));
-    CK(dalloc(c, c->ch_an, (size_t)nb));
-    CK(dalloc(c, c->ch_flags, (size_t)nb));
-    CK(dalloc(c, c->ch_status, (size_t)nb));
 
     /* one stream-ordered block for the staged caller arrays and the
        temporaries, carved in 256-byte aligned pieces */
@@ -1501,7 +1534,11 @@ static int upload_device(fn_ctx* c, int n_networks, const fn_network_desc* nets)
                  o_fl = take(nb), o_fa = take(nb), o_bad = take(4);
     StreamScratch sc;
     sc.s = c->stream;
-    CK(cudaMallocAsync(&sc.p, off, c->stream));
+    {
+        cudaMemPool_t pool;
+        CK(device_pool(c->cfg.device, &pool));
+        CK(cudaMallocFromPoolAsync(&sc.p, off, pool, c->stream));
+    }
     char* base = static_cast<char*>(sc.p);
     auto at = [&](size_t o) { return (void*)(base + o); };
 
@@ -1562,6 +1599,23 @@ static int upload_device(fn_ctx* c, int n_networks, const fn_network_desc* nets)
         CK(cp(o_th, ab, an, 8, d.a_theta0));
         CK(cp(o_ak, ab, an, 8, d.a_k));
     }
+    /* the model's device buffers while those copies run */
+    {
+        std::string what;
+        cudaError_t e = alloc_model(c, nb, ns, na, ncells, n_networks, what);
+        if (e != cudaSuccess)
+            return fail(c, e == cudaErrorMemoryAllocation ? FN_ERR_OOM : FN_ERR_CUDA,
+                        what + ": " + cudaGetErrorString(e));
+    }
+    CK(dalloc(c, c->inv_d, (size_t)nb));
+    CK(dalloc(c, c->export_xyz, (size_t)(3 * nb)));
+    CK(dalloc(c, c->perm_d, (size_t)nb));
+    CK(dalloc(c, c->sp_bead_d, (size_t)ns));
+    CK(dalloc(c, c->an_bead_d, (size_t)na));
+    CK(dalloc(c, c->ch_sp, (size_t)nb));
+    CK(dalloc(c, c->ch_an, (size_t)nb));
+    CK(dalloc(c, c->ch_flags, (size_t)nb));
+    CK(dalloc(c, c->ch_status, (size_t)nb));
     CK(cudaMemcpyAsync(at(o_nets), un.data(), sizeof(fn::UpNet) * n_networks, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(at(o_chk), chk.data(), sizeof(fn::UpCheck) * n_networks, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(at(o_link), 0, (size_t)nb, c->stream));
@@ -1685,6 +1739,8 @@ static int upload_device(fn_ctx* c, int n_networks, const fn_network_desc* nets)
     c->chain = true;
     c->host_stale = true; /* host copies of the numbering and the bonds: on first need */
     c->uploaded_on_device = true;
+    r = build_bricks(c);
+    if (r) return r;
     r = set_block(c, c->cfg.block_size > 0 ? c->cfg.block_size : 128, c->cfg.chain_mode == 0 ? kDefaultItemsPerThread : 0);
     if (r) return r;
     r = verlet_setup(c);
@@ -2358,7 +2414,8 @@ FN_API int fn_kernel_time(fn_ctx* c, double* step_ms, long long* launches, doubl
    staged chain kernel, contact items per thread and round (0: the plain chain
    kernel) -- the same `steps_per_trial` steps run from one snapshot of the
    state (restored after every trial, so the simulation does not advance),
-   timed with CUDA events; the fastest shape is kept. */
+   timed with CUDA events; the fastest shape is kept, then the faster list
+   build (by bricks or bead by bead) at that shape. */
 FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     FN_TRY
     fnh::NvtxRange nvtx_range_("fn_autotune");
@@ -2429,6 +2486,29 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
             best = sh;
         }
     }
+    /* then the list build (by bricks or bead by bead) at that shape */
+    bool best_bricks = c->list_bricks;
+    if (!r && (r = set_block(c, best.first, best.second)) == 0) {
+        float ms_build[2] = {1e30f, 1e30f};
+        for (int bricks = 0; bricks < 2 && !r; ++bricks) {
+            c->list_bricks = bricks == 1;
+            drop_graphs(c);
+            for (int rep = 0; rep < 2 && !r; ++rep) {
+                c->cur = cur0;
+                for (auto& sn : snaps)
+                    CK(cudaMemcpyAsync(const_cast<void*>(sn.src), sn.p, sn.bytes, cudaMemcpyDeviceToDevice, c->stream));
+                CK(cudaEventRecord(e0, c->stream));
+                r = fn_step(c, steps_per_trial);
+                CK(cudaEventRecord(e1, c->stream));
+            }
+            if (r) break;
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&ms_build[bricks], e0, e1));
+        }
+        best_bricks = ms_build[1] < ms_build[0];
+    }
+    c->list_bricks = best_bricks;
+    drop_graphs(c);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->cur = cur0;
@@ -2442,6 +2522,21 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     c->timing = timing0;
     if (r) return r;
     return set_block(c, best.first, best.second);
+    FN_CATCH(c)
+}
+
+/* Chooses how contact lists are built: 1 by bricks of cells staged in shared
+   memory, 0 bead by bead from global memory.  Same lists either way. */
+FN_API int fn_set_list_build(fn_ctx* c, int bricks) {
+    FN_TRY
+    int r = check_ready(c);
+    if (r) return r;
+    if (bricks != 0 && bricks != 1) return fail(c, FN_ERR_ARG, "fn_set_list_build: 0 or 1");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->list_bricks = bricks == 1;
+    return FN_OK;
     FN_CATCH(c)
 }
 

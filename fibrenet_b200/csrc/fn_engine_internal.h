@@ -105,6 +105,12 @@ struct fn_ctx {
     DevBuf<int> csr, tile_items;
     DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
     DevBuf<int> scan_sums;
+    /* staged list build: bricks of cells (network, first cell x, y, z);
+       list_bricks false (the default: measured faster) selects the per-bead
+       build */
+    DevBuf<int4> bricks;
+    int nbricks = 0;
+    bool list_bricks = false;
     DevBuf<FnTile> tiles;
     DevBuf<FnNet> nets;
     DevBuf<FnPair> pairs;
@@ -197,19 +203,35 @@ struct NvtxRange {
                                std::string(#call) + ": " + cudaGetErrorString(e_));       \
     } while (0)
 
+/* The library's stream-ordered memory pool on `device`, created on first
+   use.  Every context buffer comes from it and goes back to it: freed memory
+   stays with the pool for the next allocation (of this or a later context in
+   the process) instead of returning to the driver, so creating and
+   uploading contexts one after another does not pay the device's allocation
+   cost each time. */
+cudaError_t device_pool(int device, cudaMemPool_t* pool);
+
+/* An allocation is ordered on the context's stream: work on other streams
+   (or synchronous copies) may touch it only after that stream has been
+   synchronised, as every entry point does before returning. */
 template <class T>
 cudaError_t dalloc(fn_ctx* c, DevBuf<T>& b, size_t n) {
     if (b.p) {
-        cudaFree(b.p);
+        cudaFreeAsync(b.p, c->stream);
         c->device_bytes -= (long long)(b.n * sizeof(T));
         b.p = nullptr;
         b.n = 0;
     }
     size_t bytes = sizeof(T) * (n ? n : 1);
-    cudaError_t e = cudaMalloc((void**)&b.p, bytes);
+    cudaMemPool_t pool;
+    cudaError_t e = device_pool(c->cfg.device, &pool);
+    if (e != cudaSuccess) return e;
+    e = cudaMallocFromPoolAsync((void**)&b.p, bytes, pool, c->stream);
     if (e == cudaSuccess) {
         b.n = n ? n : 1;
         c->device_bytes += (long long)bytes;
+    } else {
+        b.p = nullptr;
     }
     return e;
 }
@@ -217,7 +239,7 @@ cudaError_t dalloc(fn_ctx* c, DevBuf<T>& b, size_t n) {
 template <class T>
 void dfree(fn_ctx* c, DevBuf<T>& b) {
     if (b.p) {
-        cudaFree(b.p);
+        cudaFreeAsync(b.p, c->stream);
         c->device_bytes -= (long long)(b.n * sizeof(T));
     }
     b.p = nullptr;

@@ -1384,6 +1384,8 @@ __device__ __forceinline__ void scan_run(const RebuildArgs& R, const FnNet& N, i
    waits on dependent loads, and the extra resident warps hide more of that
    latency than the spills cost (measured: 0.355 vs 0.373 ms per 1M-bead
    rebuild at the 54 registers the compiler picks unbounded). */
+__device__ __forceinline__ void list_one_bead(const RebuildArgs& R, const FnNet& N, int i, int c);
+
 __global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long long ncells) {
     FN_GATED(R.gate);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1391,7 +1393,12 @@ __global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long lon
     const int i = R.cell_beads[t];
     const int c = R.cell_of[i];
     if (c < 0) return; /* beyond its cell's capacity: listed nowhere */
-    const FnNet& N = R.nets[net_of_bead(R.nets, R.n_nets, i)];
+    list_one_bead(R, R.nets[net_of_bead(R.nets, R.n_nets, i)], i, c);
+}
+
+/* Bead i's full list, reading its candidates from global memory (k_lists,
+   and bricks with more candidates than their shared memory holds). */
+__device__ __forceinline__ void list_one_bead(const RebuildArgs& R, const FnNet& N, int i, int c) {
     const double4 pi = R.pos[i];
     const int4 bi = R.binfo[i];
     const int lc = c - N.cell_base;
@@ -1440,6 +1447,174 @@ __global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long lon
     if (n > R.list_cap)
         atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
     R.list_count[i] = n;
+}
+
+/* BuildContactList by bricks of cells (the same lists as k_lists, entry for
+   entry): one block per brick of kBrickX x kBrickY x kBrickZ cells of one
+   network.  The block stages, once, every listable bead of the brick's cells
+   and of the cells around them (ids, positions and bead info, in cell order:
+   halo rows z-major, then y, then x, beads ascending within a cell, the first
+   cell_cap of a full cell), in three wide rounds of loads -- cell counts and
+   starts, bead ids, then positions and bead info by cp.async -- instead of a
+   chain of dependent loads per candidate.  Each bead of the brick then scans
+   its 27 cells from shared memory in k_lists' order (dz, dy, dx ascending),
+   so the lists are k_lists' lists.  A brick whose halo holds more than
+   kBrickCands beads lists its beads from global memory (list_one_bead). */
+constexpr int kBrickHalo = (kBrickX + 2) * (kBrickY + 2) * (kBrickZ + 2);
+constexpr int kBrickCells = kBrickX * kBrickY * kBrickZ;
+constexpr int kBrickThreads = 128;
+
+/* last index h of a[0..n] with a[h] <= q (a non-decreasing, a[0] <= q) */
+__device__ __forceinline__ int last_le(const int* a, int n, int q) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a[mid] <= q)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+/* exclusive scan of v[0..n) into out[0..n] (out[n] the total) by one block */
+__device__ __forceinline__ void block_scan_array(const int* v, int n, int* out, int* ws) {
+    const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int b = threadIdx.x * per, e = min(b + per, n);
+    int sum = 0;
+    for (int k = b; k < e; ++k) sum += v[k];
+    int total;
+    int acc = block_scan_any(sum, ws, total);
+    for (int k = b; k < e; ++k) {
+        out[k] = acc;
+        acc += v[k];
+    }
+    if (threadIdx.x == 0) out[n] = total;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBrickThreads) k_lists_brick(const RebuildArgs R, const int4* __restrict__ bricks) {
+    FN_GATED(R.gate);
+    __shared__ int s_cnt[kBrickHalo], s_start[kBrickHalo], s_coff[kBrickHalo + 1];
+    __shared__ int s_icnt[kBrickCells], s_ioff[kBrickCells + 1];
+    __shared__ int s_ws[33];
+    __shared__ int s_id[kBrickCands];
+    __shared__ double4 s_pos[kBrickCands];
+    __shared__ int4 s_bin[kBrickCands];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int4 B = bricks[blockIdx.x]; /* network, first cell x, y, z */
+    const FnNet& N = R.nets[B.x];
+    const int ex = min(kBrickX, N.nx - B.y), ey = min(kBrickY, N.ny - B.z), ez = min(kBrickZ, N.nz - B.w);
+    const int HX = ex + 2, HY = ey + 2, H = HX * HY * (ez + 2), NIC = ex * ey * ez;
+    /* round 1: count (first cell_cap of a full cell) and start of every halo
+       cell; a cell off a non-periodic side holds nothing */
+    for (int hc = tid; hc < H; hc += nt) {
+        const int hx = hc % HX, hy = (hc / HX) % HY, hz = hc / (HX * HY);
+        int gx = B.y - 1 + hx, gy = B.z - 1 + hy, gz = B.w - 1 + hz;
+        bool ok = true;
+        if (gx < 0 || gx >= N.nx) {
+            if (N.periodic & 1)
+                gx = gx < 0 ? N.nx - 1 : 0;
+            else
+                ok = false;
+        }
+        if (gy < 0 || gy >= N.ny) {
+            if (N.periodic & 2)
+                gy = gy < 0 ? N.ny - 1 : 0;
+            else
+                ok = false;
+        }
+        if (gz < 0 || gz >= N.nz) {
+            if (N.periodic & 4)
+                gz = gz < 0 ? N.nz - 1 : 0;
+            else
+                ok = false;
+        }
+        int cnt = 0, st = 0;
+        if (ok) {
+            const int cell = N.cell_base + gx + gy * N.nx + gz * N.nxy;
+            cnt = min(R.cell_count[cell], R.cell_cap);
+            st = R.cell_start[cell];
+        }
+        s_cnt[hc] = cnt;
+        s_start[hc] = st;
+    }
+    __syncthreads();
+    for (int ic = tid; ic < NIC; ic += nt) {
+        const int ix = ic % ex, iy = (ic / ex) % ey, iz = ic / (ex * ey);
+        s_icnt[ic] = s_cnt[((iz + 1) * HY + (iy + 1)) * HX + (ix + 1)];
+    }
+    __syncthreads();
+    block_scan_array(s_cnt, H, s_coff, s_ws);
+    block_scan_array(s_icnt, NIC, s_ioff, s_ws);
+    const int C = s_coff[H], NI = s_ioff[NIC];
+    if (C > kBrickCands) {
+        /* too many to stage: each bead from global memory */
+        for (int u = tid; u < NI; u += nt) {
+            const int ic = last_le(s_ioff, NIC, u);
+            const int ix = ic % ex, iy = (ic / ex) % ey, iz = ic / (ex * ey);
+            const int hc = ((iz + 1) * HY + (iy + 1)) * HX + (ix + 1);
+            const int i = R.cell_beads[s_start[hc] + (u - s_ioff[ic])];
+            list_one_bead(R, N, i, R.cell_of[i]);
+        }
+        return;
+    }
+    /* round 2: bead ids; round 3: their positions and bead info */
+    constexpr int kPer = (kBrickCands + kBrickThreads - 1) / kBrickThreads;
+    int ids[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int q = tid + k * nt;
+        ids[k] = -1;
+        if (q < C) {
+            const int hc = last_le(s_coff, H, q);
+            ids[k] = R.cell_beads[s_start[hc] + (q - s_coff[hc])];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int q = tid + k * nt;
+        if (q < C && ids[k] >= 0) {
+            s_id[q] = ids[k];
+            const uint32_t dp = smem_addr(s_pos + q), db = smem_addr(s_bin + q);
+            cp_async16(dp, R.pos + ids[k]);
+            cp_async16(dp + 16, reinterpret_cast<const char*>(R.pos + ids[k]) + 16);
+            cp_async16(db, R.binfo + ids[k]);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int u = tid; u < NI; u += nt) {
+        const int ic = last_le(s_ioff, NIC, u);
+        const int ix = ic % ex, iy = (ic / ex) % ey, iz = ic / (ex * ey);
+        const int q = s_coff[((iz + 1) * HY + (iy + 1)) * HX + (ix + 1)] + (u - s_ioff[ic]);
+        const int i = s_id[q];
+        const double4 pi = s_pos[q];
+        const int4 bi = s_bin[q];
+        int* __restrict__ out = R.list + i;
+        int n = 0;
+        for (int dz = 0; dz < 3; ++dz)
+            for (int dy = 0; dy < 3; ++dy) {
+                const int row = ((iz + dz) * HY + (iy + dy)) * HX + ix; /* halo cell of dx = -1 */
+                const int q1 = s_coff[row + 3];
+                for (int qq = s_coff[row]; qq < q1; ++qq) {
+                    const int j = s_id[qq];
+                    if (j == i) continue;
+                    const double4 pj = s_pos[qq];
+                    double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+                    double length = rx * rx + ry * ry + rz * rz;
+                    if (N.list_mi) length = min_image(N, rx, ry, rz, length, N.list_mi);
+                    if (!(length < N.list_r2_max)) continue; /* listed by no pair kind */
+                    if (list_accept(N, R.pairs, length, pi, bi, pj, s_bin[qq])) {
+                        if (n < R.list_cap) out[(size_t)n * R.list_stride] = j;
+                        ++n;
+                    }
+                }
+            }
+        if (n > R.list_cap)
+            atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
+        R.list_count[i] = n;
+    }
 }
 
 /* Tile-compacted copy of the contact list for the staged step kernel: tile
@@ -1835,8 +2010,12 @@ cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, 
     } else {
         if ((e = cudaMemsetAsync(R.list_count, 0, sizeof(int) * (size_t)nb, s))) return e;
     }
-    /* every bead may sit in the grid; threads past the grid total return */
-    if (nb > 0) k_lists<<<(nb + 127) / 128, 128, 0, s>>>(R, ncells);
+    if (R.bricks) {
+        if (R.nbricks > 0) k_lists_brick<<<R.nbricks, kBrickThreads, 0, s>>>(R, R.bricks);
+    } else if (nb > 0) {
+        /* every bead may sit in the grid; threads past the grid total return */
+        k_lists<<<(nb + 127) / 128, 128, 0, s>>>(R, ncells);
+    }
     /* the staged step kernel's copy, one block per tile (tiles are at most
        block - 4 beads wide) */
     if (R.csr && ntiles > 0) k_list_tiles<<<ntiles, block, 0, s>>>(R);

@@ -188,6 +188,10 @@ __host__ __device__ inline StagedSmem staged_smem_layout(int block, int chunk) {
 
 inline size_t step_staged_smem(int block, int chunk) { return staged_smem_layout(block, chunk).total; }
 
+/* bricks of the staged list build: cells per brick along x, y, z, and the
+   most halo beads a brick stages in shared memory */
+constexpr int kBrickX = 8, kBrickY = 4, kBrickZ = 4, kBrickCands = 512;
+
 struct RebuildArgs {
     const FnTile* tiles;
     const FnNet* nets;
@@ -207,6 +211,10 @@ struct RebuildArgs {
     unsigned long long* counters;
     int n_nets;
     const int* gate; /* displacement mode: rebuild only when *gate != 0 */
+    /* bricks of the staged list build: network, first cell x, y, z (null:
+       the per-bead list build) */
+    const int4* bricks;
+    int nbricks;
     /* tile-compacted copy of the list for the staged step kernel (null: none) */
     int* csr;
     long long csr_region;

@@ -121,6 +121,7 @@ SIGNATURES = {
     "fn_forces_only": (C.c_int, [C.c_void_p, C.c_int]),
     "fn_autotune": (C.c_int, [C.c_void_p, C.c_int]),
     "fn_set_kernel_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "fn_set_list_build": (C.c_int, [C.c_void_p, C.c_int]),
     "fn_state_save": (C.c_int, [C.c_void_p]),
     "fn_state_restore": (C.c_int, [C.c_void_p]),
     "fn_step_timed": (C.c_int, [C.c_void_p, C.c_int, _D]),
@@ -443,6 +444,10 @@ class Simulation:
         """Step-kernel shape: block size and, for the staged chain kernel,
         contact items per thread and round (0: no staging)."""
         self._check(self.lib.fn_set_kernel_shape(self.h, int(block), int(items_per_thread)))
+
+    def set_list_build(self, bricks: bool) -> None:
+        """Contact lists by bricks of cells (True) or bead by bead (False, the default)."""
+        self._check(self.lib.fn_set_list_build(self.h, int(bool(bricks))))
 
     def autotune(self, steps_per_trial: int = 20) -> int:
         self._check(self.lib.fn_autotune(self.h, steps_per_trial))

@@ -354,9 +354,17 @@ FN_API int fn_device_view(fn_ctx* ctx, int field, fn_view* out);
 /* Times steps_per_trial steps at each candidate shape of the step kernel
    (block size 64 .. 512; for the staged chain kernel also 2, 4 or 8 contact
    items per thread and round, or no staging) from one snapshot of the state,
-   restored after every trial, and keeps the fastest; the simulation does not
+   restored after every trial, keeps the fastest, then keeps the faster of the
+   two list builds (fn_set_list_build) at that shape; the simulation does not
    advance. */
 FN_API int fn_autotune(fn_ctx* ctx, int steps_per_trial);
+
+/* How contact lists are built (ResetGrid .. BuildContactList,
+   kernel.cl:487-789): 1 by bricks of 8 x 4 x 4 grid cells whose beads and
+   neighbouring beads are staged in shared memory, 0 (the default) bead by
+   bead from global memory.  Both give the same lists, entry for entry;
+   fn_autotune keeps the faster. */
+FN_API int fn_set_list_build(fn_ctx* ctx, int bricks);
 
 /* Sets the step kernel's shape: threads per block (a multiple of 32; 64 ..
    256 on the chain path, whose tiles hold block - 4 beads) and, for the

@@ -44,6 +44,11 @@ static inline cudaError_t hu_attr(int* v) {
     *v = 227 * 1024; /* a B200's opt-in shared memory per block */
     return cudaSuccess;
 }
+static inline cudaError_t hu_pool(cudaMemPool_t* p) {
+    static int token;
+    *p = reinterpret_cast<cudaMemPool_t>(&token);
+    return cudaSuccess;
+}
 static inline cudaError_t hu_stream(cudaStream_t* s) {
     *s = nullptr;
     return cudaSuccess;
@@ -60,6 +65,9 @@ static inline cudaError_t hu_stream(cudaStream_t* s) {
 #define cudaMalloc(p, n) hu_malloc((void**)(p), n)
 #define cudaFree(p) hu_free((void*)(p))
 #define cudaMallocAsync(p, n, st) hu_malloc((void**)(p), n)
+#define cudaMallocFromPoolAsync(p, n, pl, st) hu_malloc((void**)(p), n)
+#define cudaMemPoolCreate(pl, props) hu_pool(pl)
+#define cudaMemPoolSetAttribute(pl, a, v) hu_ok()
 #define cudaFreeAsync(p, st) hu_free((void*)(p))
 #define cudaMemcpyAsync(d, s, n, k, st) hu_copy(d, s, n)
 #define cudaMemcpy(d, s, n, k) hu_copy(d, s, n)
