@@ -246,6 +246,15 @@ def traffic_from_profiles():
     return None
 
 
+def traffic_bytes(m):
+    """DRAM bytes of one step launch (ncu capture of the tensile network),
+    for the 1M-bead tensile workload only; null for other networks."""
+    per = traffic_from_profiles()
+    if per is None or m.n_beads != 1_000_000 or int(m.meta.get("beads", 0)) != 50 or m.n_types != 3:
+        return None
+    return per * m.n_beads
+
+
 def rebuilds_per_call(K: int, freq: int) -> int:
     """Contact rebuilds of one fn_step(K) call: at step 0 and every freq steps
     (the counter restarts with every call, SimulationManager.cpp:152)."""
@@ -489,7 +498,10 @@ def headline(args, m, world, rank, local, dist, e2e=True, cpu=True, label=None):
                        "algorithmic_bytes_per_launch": alg,
                        "layout_bytes_per_launch": layout_bytes(m, half_pairs, stats["bond_path"] == 2),
                        "step_kernel_ms": step_ms, "rebuild_ms": kt["rebuild_ms"],
-                       "whole_step_frac": alg / (med / K / 1e3) / 1e9 / peak}
+                       "whole_step_frac": alg / (med / K / 1e3) / 1e9 / peak,
+                       "traffic": traffic_bytes(m),
+                       "traffic_source": "profiles/k_step_tensile_traffic.txt (ncu dram__bytes_read.sum + "
+                                         "dram__bytes_write.sum of one step launch on this network)"}
     sim.close()
 
     if e2e and not args.no_e2e:
@@ -723,6 +735,7 @@ def run_ours(args):
             "data": "synthetic (seeded generator; reference ships no models)",
             "config": config_dict(m, args, {"half_list_pairs": r["half_pairs"], "block_size": r["block"],
                                             "items_per_thread": r["stats"]["items_per_thread"],
+                                            "list_build": "bricks" if r["stats"]["list_by_bricks"] else "beads",
                                             "storage": "positions f64, velocities/forces f32",
                                             "timed_region": f"fn_step({args.steps}) from one saved state, "
                                                             f"{r['reps']} repetitions, median"}),

@@ -2283,6 +2283,7 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     out->block_size = c->block;
     out->items_per_thread = c->staged ? c->chunk / c->block : 0;
     out->upload_on_device = c->uploaded_on_device ? 1 : 0;
+    out->list_by_bricks = c->list_bricks ? 1 : 0;
     out->bond_path = c->chain ? 2 : (c->tiled ? 1 : 0);
     out->graph_launches = c->graph_launches;
     out->n_networks = c->n_nets;

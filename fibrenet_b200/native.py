@@ -56,7 +56,7 @@ class FnStats(C.Structure):
                 ("bond_path", C.c_int), ("n_networks", C.c_int), ("n_beads", C.c_longlong),
                 ("device_bytes", C.c_longlong), ("graph_launches", C.c_longlong),
                 ("nonfinite", C.c_longlong), ("items_per_thread", C.c_int),
-                ("stalls", C.c_longlong), ("upload_on_device", C.c_int)]
+                ("stalls", C.c_longlong), ("upload_on_device", C.c_int), ("list_by_bricks", C.c_int)]
 
 
 class FnView(C.Structure):

@@ -157,6 +157,8 @@ typedef struct fn_stats {
                                   staged data ran out (fn_sync then fails) */
     int upload_on_device;      /* 1: the last fn_upload checked, ordered and
                                   converted the model on the device */
+    int list_by_bricks;        /* 1: contact lists built by bricks of cells
+                                  (fn_set_list_build) */
 } fn_stats;
 
 /* A device array of the context, for zero-copy readers (torch through
