@@ -1386,14 +1386,112 @@ __device__ __forceinline__ void scan_run(const RebuildArgs& R, const FnNet& N, i
    rebuild at the 54 registers the compiler picks unbounded). */
 __device__ __forceinline__ void list_one_bead(const RebuildArgs& R, const FnNet& N, int i, int c);
 
+/* Runs of consecutive candidates a thread of k_lists keeps in shared memory
+   (a row of three cells is one run unless it wraps or a cell is full). */
+constexpr int kListRuns = 12;
+
 __global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long long ncells) {
     FN_GATED(R.gate);
+    __shared__ int2 s_runs[128 * kListRuns];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= R.cell_start[ncells]) return; /* beads placed in the grid */
     const int i = R.cell_beads[t];
     const int c = R.cell_of[i];
     if (c < 0) return; /* beyond its cell's capacity: listed nowhere */
-    list_one_bead(R, R.nets[net_of_bead(R.nets, R.n_nets, i)], i, c);
+    const FnNet& N = R.nets[net_of_bead(R.nets, R.n_nets, i)];
+    /* the bead's candidates as runs of the sorted bead array, in list order
+       (dz, dy, dx ascending, beads ascending within a cell) */
+    int2* runs = s_runs + threadIdx.x * kListRuns;
+    int nr = 0;
+    bool spill = false;
+    const int lc = c - N.cell_base;
+    const int cz = lc / N.nxy;
+    const int cy = (lc - cz * N.nxy) / N.nx;
+    const int cx = lc - cz * N.nxy - cy * N.nx;
+    for (int dz = -1; dz <= 1 && !spill; ++dz) {
+        int z = cz + dz;
+        if (z < 0 || z >= N.nz) {
+            if (!(N.periodic & 4)) continue;
+            z = z < 0 ? N.nz - 1 : 0;
+        }
+        for (int dy = -1; dy <= 1 && !spill; ++dy) {
+            int y = cy + dy;
+            if (y < 0 || y >= N.ny) {
+                if (!(N.periodic & 2)) continue;
+                y = y < 0 ? N.ny - 1 : 0;
+            }
+            const int row = N.cell_base + y * N.nx + z * N.nxy;
+            if (cx >= 1 && cx + 1 < N.nx) {
+                const int c0 = row + cx - 1;
+                const int s0 = R.cell_start[c0];
+                const int s3 = R.cell_start[c0 + 3];
+                if (s3 - s0 <= R.cell_cap ||
+                    (R.cell_count[c0] <= R.cell_cap && R.cell_count[c0 + 1] <= R.cell_cap &&
+                     R.cell_count[c0 + 2] <= R.cell_cap)) {
+                    if (s3 > s0) {
+                        if (nr == kListRuns) {
+                            spill = true;
+                            break;
+                        }
+                        runs[nr++] = make_int2(s0, s3 - s0);
+                    }
+                    continue;
+                }
+            }
+            for (int dx = -1; dx <= 1; ++dx) {
+                int x = cx + dx;
+                if (x < 0 || x >= N.nx) {
+                    if (!(N.periodic & 1)) continue;
+                    x = x < 0 ? N.nx - 1 : 0;
+                }
+                const int nc = row + x;
+                int m = R.cell_count[nc];
+                if (m > R.cell_cap) m = R.cell_cap;
+                if (m > 0) {
+                    if (nr == kListRuns) {
+                        spill = true;
+                        break;
+                    }
+                    runs[nr++] = make_int2(R.cell_start[nc], m);
+                }
+            }
+        }
+    }
+    if (spill) { /* more runs than the table holds: the row-by-row scan */
+        list_one_bead(R, N, i, c);
+        return;
+    }
+    /* one loop over all runs, so a warp iterates as often as its busiest lane
+       has candidates, not as often as the sum of each row's busiest lane */
+    const double4 pi = R.pos[i];
+    const int4 bi = R.binfo[i];
+    int* __restrict__ out = R.list + i;
+    int n = 0;
+    int r = 0, q = 0, qe = 0;
+    if (nr > 0) {
+        q = runs[0].x;
+        qe = q + runs[0].y;
+    }
+    while (r < nr) {
+        const int j = R.cell_beads[q];
+        if (j != i) {
+            const double4 pj = R.pos[j];
+            double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+            double length = rx * rx + ry * ry + rz * rz;
+            if (N.list_mi) length = min_image(N, rx, ry, rz, length, N.list_mi);
+            if (length < N.list_r2_max && list_accept(N, R.pairs, length, pi, bi, pj, R.binfo[j])) {
+                if (n < R.list_cap) out[(size_t)n * R.list_stride] = j;
+                ++n;
+            }
+        }
+        if (++q == qe && ++r < nr) {
+            q = runs[r].x;
+            qe = q + runs[r].y;
+        }
+    }
+    if (n > R.list_cap)
+        atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
+    R.list_count[i] = n;
 }
 
 /* Bead i's full list, reading its candidates from global memory (k_lists,
