@@ -95,3 +95,17 @@ def test_full_lists_counted_like_the_mirror(oracle_built):
     assert s.stats()["list_overflow"] > 0
     assert s.stats()["list_overflow"] == o.overflow()[1]
     s.close()
+
+
+@pytest.mark.parametrize("cap", [1, 2, 3])
+def test_chain_path_under_tiny_list_capacity(oracle_built, cap):
+    """Fibres on the chain bond path whose contact lists are cut to 1-3
+    entries: the GPU drops exactly the entries the mirror drops, counts them
+    alike, and the bits still agree."""
+    m = g.tensile_network(seed=5, fibres=60, beads=30, box=(60.0, 40.0, 10.0), z_range=(1.0, 9.0),
+                          clamp_lo=2.0, clamp_hi=58.0, placement="host")
+    s, o = same_as_mirror(m, [8, 8, 3], list_cap=cap)
+    assert s.stats()["bond_path"] == 2
+    assert s.stats()["list_overflow"] > 0
+    assert s.stats()["list_overflow"] == o.overflow()[1]
+    s.close()
