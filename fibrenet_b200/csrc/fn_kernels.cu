@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "fn_detmath.h"
 #include "fn_device.cuh"
@@ -1303,6 +1304,27 @@ __global__ void k_cell_sort(const RebuildArgs R, int ncells) {
     const int n = R.cell_count[c];
     if (n <= 1) return;
     int* b = R.cell_beads + R.cell_start[c];
+    if (n <= 8 && n <= R.cell_cap) {
+        /* the common case (about one bead per cell): sorted in registers by
+           Batcher's 8-input network, absent slots holding INT_MAX */
+        int v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = k < n ? b[k] : INT_MAX;
+        constexpr int net[19][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6},
+                                    {5, 7}, {1, 2}, {5, 6}, {0, 4}, {1, 5}, {2, 6}, {3, 7},
+                                    {2, 4}, {3, 5}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const int lo = min(v[net[q][0]], v[net[q][1]]);
+            const int hi = max(v[net[q][0]], v[net[q][1]]);
+            v[net[q][0]] = lo;
+            v[net[q][1]] = hi;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k < n) b[k] = v[k];
+        return;
+    }
     /* selection of the first min(n, cap) positions: ascending order there,
        O(cap * n) even for an overfull cell */
     const int keep = n < R.cell_cap ? n : R.cell_cap;
