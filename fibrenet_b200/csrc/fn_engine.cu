@@ -1687,19 +1687,30 @@ static int upload_device(fn_ctx* c, int n_networks, const fn_network_desc* nets)
         CK(cudaMemcpyAsync(ky.data(), key, sizeof(unsigned long long) * (size_t)n_runs, cudaMemcpyDeviceToHost,
                            c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        std::vector<int> out(n_runs);
+        std::vector<int> out(n_runs), ord(n_runs), tmp(n_runs);
         int r0 = 0;
         for (int k = 0; k < n_networks; ++k) {
             const int bb = c->info[k].bead_begin, be = c->info[k].bead_end;
             int r1 = r0;
             while (r1 < n_runs && st[r1] < be) ++r1;
-            std::vector<unsigned long long> sorted(ky.begin() + r0, ky.begin() + r1);
-            std::sort(sorted.begin(), sorted.end());
+            /* the runs by key: the key's low word is the run's first bead,
+               which grows with the run index, so a stable sort of the runs
+               (in index order) by the 30-bit Morton code in the high word
+               gives the order of a sort of the whole keys -- three passes of
+               a 10-bit counting sort */
+            for (int q = r0; q < r1; ++q) ord[q] = q;
+            for (int pass = 0; pass < 3; ++pass) {
+                const int shift = 32 + 10 * pass;
+                int count[1025] = {0};
+                for (int q = r0; q < r1; ++q) ++count[((ky[ord[q]] >> shift) & 1023) + 1];
+                for (int v = 0; v < 1024; ++v) count[v + 1] += count[v];
+                for (int q = r0; q < r1; ++q) tmp[r0 + count[(ky[ord[q]] >> shift) & 1023]++] = ord[q];
+                std::copy(tmp.begin() + r0, tmp.begin() + r1, ord.begin() + r0);
+            }
             int acc = bb;
-            for (unsigned long long kk : sorted) {
-                const int first = bb + (int)(uint32_t)kk;
-                const int rr = (int)(std::lower_bound(st.begin() + r0, st.begin() + r1, first) - st.begin());
-                const int len = (rr + 1 < r1 ? st[rr + 1] : be) - first;
+            for (int q = r0; q < r1; ++q) {
+                const int rr = ord[q];
+                const int len = (rr + 1 < r1 ? st[rr + 1] : be) - st[rr];
                 out[rr] = acc;
                 acc += len;
             }
