@@ -21,7 +21,7 @@ from gpu_util import FIELDS, rel_norm, run_seq
 
 pytestmark = pytest.mark.gpu
 
-FORCE_TOL = 1e-5  # relative, norm-wise, FP32 result vs FP64 reference
+FORCE_TOL = 1e-5  # relative, norm-wise, FP32 result vs FP64 reference (the per-step force bound)
 
 
 def sim(model, **kw):
