@@ -1405,7 +1405,8 @@ __device__ __forceinline__ void scan_run(const RebuildArgs& R, const FnNet& N, i
 /* 12 blocks of 128 per SM (at most 40 registers, a few spilled): the scan
    waits on dependent loads, and the extra resident warps hide more of that
    latency than the spills cost (measured: 0.355 vs 0.373 ms per 1M-bead
-   rebuild at the 54 registers the compiler picks unbounded). */
+   rebuild at the 54 registers the compiler picks unbounded; with the single
+   candidate loop, 0.319 vs 0.327 ms at 10 blocks and 48 registers). */
 __device__ __forceinline__ void list_one_bead(const RebuildArgs& R, const FnNet& N, int i, int c);
 
 /* Runs of consecutive candidates a thread of k_lists keeps in shared memory
