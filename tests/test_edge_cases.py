@@ -109,3 +109,20 @@ def test_chain_path_under_tiny_list_capacity(oracle_built, cap):
     assert s.stats()["list_overflow"] > 0
     assert s.stats()["list_overflow"] == o.overflow()[1]
     s.close()
+
+
+@pytest.mark.parametrize("cell_cap", [1, 3, 7, 8, 9, 64])
+def test_cell_sort_paths_like_the_mirror(oracle_built, cell_cap):
+    """Cells of up to eight beads are ordered in registers, larger or overfull
+    ones by selection: a dense gas (up to ~10 beads per cell) at capacities
+    below, at and above eight keeps the mirror's cells, lists and bits."""
+    m = gas(n=2000, seed=12, side=6.0, vel=0.2)
+    s, o = same_as_mirror(m, [8, 8, 5], cell_cap=cell_cap, list_cap=256)
+    bc, cc = s.cells()
+    obc, occ = o.cells()
+    np.testing.assert_array_equal(cc, occ)
+    np.testing.assert_array_equal(bc, obc)
+    assert s.stats()["cell_overflow"] == o.overflow()[0]
+    if cell_cap <= 8:
+        assert s.stats()["cell_overflow"] > 0
+    s.close()
