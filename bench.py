@@ -745,7 +745,7 @@ def run_ours(args):
             "data": "synthetic (seeded generator; reference ships no models)",
             "config": config_dict(m, args, {"half_list_pairs": r["half_pairs"], "block_size": r["block"],
                                             "items_per_thread": r["stats"]["items_per_thread"],
-                                            "list_build": "bricks" if r["stats"]["list_by_bricks"] else "beads",
+                                            "list_build": ("beads", "bricks", "groups")[r["stats"]["list_build"]],
                                             "storage": "positions f64, velocities/forces f32",
                                             "timed_region": f"fn_step({args.steps}) from one saved state, "
                                                             f"{r['reps']} repetitions, median"}),

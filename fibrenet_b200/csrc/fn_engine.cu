@@ -870,7 +870,8 @@ fn::RebuildArgs rebuild_args(fn_ctx* c) {
     R.cell_cap = c->cfg.cell_capacity;
     R.counters = c->counters.p;
     R.n_nets = c->n_nets;
-    R.bricks = c->list_bricks ? c->bricks.p : nullptr;
+    R.bricks = c->list_build == 1 ? c->bricks.p : nullptr;
+    R.list_lanes = c->list_build == 2 ? 8 : 0;
     R.nbricks = c->nbricks;
     R.csr = c->staged ? c->csr.p : nullptr;
     R.csr_region = c->csr_region;
@@ -2294,7 +2295,8 @@ FN_API int fn_get_stats(fn_ctx* c, fn_stats* out) {
     out->block_size = c->block;
     out->items_per_thread = c->staged ? c->chunk / c->block : 0;
     out->upload_on_device = c->uploaded_on_device ? 1 : 0;
-    out->list_by_bricks = c->list_bricks ? 1 : 0;
+    out->list_by_bricks = c->list_build == 1 ? 1 : 0;
+    out->list_build = c->list_build;
     out->bond_path = c->chain ? 2 : (c->tiled ? 1 : 0);
     out->graph_launches = c->graph_launches;
     out->n_networks = c->n_nets;
@@ -2498,12 +2500,13 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
             best = sh;
         }
     }
-    /* then the list build (by bricks or bead by bead) at that shape */
-    bool best_bricks = c->list_bricks;
+    /* then the list build (bead by bead, by bricks, by groups of lanes) at
+       that shape */
+    int best_build = c->list_build;
     if (!r && (r = set_block(c, best.first, best.second)) == 0) {
-        float ms_build[2] = {1e30f, 1e30f};
-        for (int bricks = 0; bricks < 2 && !r; ++bricks) {
-            c->list_bricks = bricks == 1;
+        float ms_build[3] = {1e30f, 1e30f, 1e30f};
+        for (int mode = 0; mode < 3 && !r; ++mode) {
+            c->list_build = mode;
             drop_graphs(c);
             for (int rep = 0; rep < 2 && !r; ++rep) {
                 c->cur = cur0;
@@ -2515,11 +2518,13 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
             }
             if (r) break;
             CK(cudaEventSynchronize(e1));
-            CK(cudaEventElapsedTime(&ms_build[bricks], e0, e1));
+            CK(cudaEventElapsedTime(&ms_build[mode], e0, e1));
         }
-        best_bricks = ms_build[1] < ms_build[0];
+        best_build = 0;
+        for (int mode = 1; mode < 3; ++mode)
+            if (ms_build[mode] < ms_build[best_build]) best_build = mode;
     }
-    c->list_bricks = best_bricks;
+    c->list_build = best_build;
     drop_graphs(c);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -2537,17 +2542,18 @@ FN_API int fn_autotune(fn_ctx* c, int steps_per_trial) {
     FN_CATCH(c)
 }
 
-/* Chooses how contact lists are built: 1 by bricks of cells staged in shared
-   memory, 0 bead by bead from global memory.  Same lists either way. */
+/* Chooses how contact lists are built: 0 bead by bead from global memory, 1
+   by bricks of cells staged in shared memory, 2 by groups of 8 lanes per
+   bead.  Same lists, entry for entry, every way. */
 FN_API int fn_set_list_build(fn_ctx* c, int bricks) {
     FN_TRY
     int r = check_ready(c);
     if (r) return r;
-    if (bricks != 0 && bricks != 1) return fail(c, FN_ERR_ARG, "fn_set_list_build: 0 or 1");
+    if (bricks < 0 || bricks > 2) return fail(c, FN_ERR_ARG, "fn_set_list_build: 0, 1 or 2");
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
     drop_graphs(c);
-    c->list_bricks = bricks == 1;
+    c->list_build = bricks;
     return FN_OK;
     FN_CATCH(c)
 }

@@ -105,12 +105,12 @@ struct fn_ctx {
     DevBuf<int> csr, tile_items;
     DevBuf<int> cell_of, cell_count, cell_fill, cell_start, cell_beads, list_count, list;
     DevBuf<int> scan_sums;
-    /* staged list build: bricks of cells (network, first cell x, y, z);
-       list_bricks false (the default: measured faster) selects the per-bead
-       build */
+    /* the list build: 0 one thread per bead (the default), 1 by bricks of
+       cells (network, first cell x, y, z of each) staged in shared memory,
+       2 by groups of 8 lanes per bead */
     DevBuf<int4> bricks;
     int nbricks = 0;
-    bool list_bricks = false;
+    int list_build = 0;
     DevBuf<FnTile> tiles;
     DevBuf<FnNet> nets;
     DevBuf<FnPair> pairs;

@@ -1413,6 +1413,57 @@ __device__ __forceinline__ void list_one_bead(const RebuildArgs& R, const FnNet&
    (a row of three cells is one run unless it wraps or a cell is full). */
 constexpr int kListRuns = 12;
 
+/* Bead i's candidates (cell c) as runs of the sorted bead array, in list
+   order (dz, dy, dx ascending, beads ascending within a cell); false when
+   they take more than kListRuns runs. */
+__device__ __forceinline__ bool list_runs(const RebuildArgs& R, const FnNet& N, int c, int cz, int cy, int cx,
+                                          int2* runs, int& nr) {
+    for (int dz = -1; dz <= 1; ++dz) {
+        int z = cz + dz;
+        if (z < 0 || z >= N.nz) {
+            if (!(N.periodic & 4)) continue;
+            z = z < 0 ? N.nz - 1 : 0;
+        }
+        for (int dy = -1; dy <= 1; ++dy) {
+            int y = cy + dy;
+            if (y < 0 || y >= N.ny) {
+                if (!(N.periodic & 2)) continue;
+                y = y < 0 ? N.ny - 1 : 0;
+            }
+            const int row = N.cell_base + y * N.nx + z * N.nxy;
+            if (cx >= 1 && cx + 1 < N.nx) {
+                const int c0 = row + cx - 1;
+                const int s0 = R.cell_start[c0];
+                const int s3 = R.cell_start[c0 + 3];
+                if (s3 - s0 <= R.cell_cap ||
+                    (R.cell_count[c0] <= R.cell_cap && R.cell_count[c0 + 1] <= R.cell_cap &&
+                     R.cell_count[c0 + 2] <= R.cell_cap)) {
+                    if (s3 > s0) {
+                        if (nr == kListRuns) return false;
+                        runs[nr++] = make_int2(s0, s3 - s0);
+                    }
+                    continue;
+                }
+            }
+            for (int dx = -1; dx <= 1; ++dx) {
+                int x = cx + dx;
+                if (x < 0 || x >= N.nx) {
+                    if (!(N.periodic & 1)) continue;
+                    x = x < 0 ? N.nx - 1 : 0;
+                }
+                const int nc = row + x;
+                int m = R.cell_count[nc];
+                if (m > R.cell_cap) m = R.cell_cap;
+                if (m > 0) {
+                    if (nr == kListRuns) return false;
+                    runs[nr++] = make_int2(R.cell_start[nc], m);
+                }
+            }
+        }
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long long ncells) {
     FN_GATED(R.gate);
     __shared__ int2 s_runs[128 * kListRuns];
@@ -1515,6 +1566,89 @@ __global__ void __launch_bounds__(128, 12) k_lists(const RebuildArgs R, long lon
     if (n > R.list_cap)
         atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
     R.list_count[i] = n;
+}
+
+/* BuildContactList with G lanes per bead (the same lists as k_lists, entry
+   for entry), for networks too small to hide k_lists' chain of dependent
+   loads with one thread per bead: a bead's candidates are taken G at a time,
+   lane l of its group testing candidate (round x G + l), and the accepted
+   ones are written in candidate order by a ballot over the group.  Blocks
+   of 128 threads, 128 / G beads in cell order. */
+template <int G>
+__global__ void __launch_bounds__(128) k_lists_group(const RebuildArgs R, long long ncells) {
+    FN_GATED(R.gate);
+    constexpr int PER = 128 / G;
+    __shared__ int2 s_runs[PER * kListRuns];
+    __shared__ int s_nr[PER];
+    const int lane = threadIdx.x & 31, gl = threadIdx.x % G, grp = threadIdx.x / G;
+    const int t = blockIdx.x * PER + grp;
+    int i = -1, c = -1;
+    if (t < R.cell_start[ncells]) { /* beads placed in the grid */
+        i = R.cell_beads[t];
+        c = R.cell_of[i];
+        if (c < 0) i = -1; /* beyond its cell's capacity: listed nowhere */
+    }
+    const FnNet& N = R.nets[i >= 0 ? net_of_bead(R.nets, R.n_nets, i) : 0];
+    int2* runs = s_runs + grp * kListRuns;
+    if (gl == 0) {
+        int nr = 0;
+        if (i >= 0) {
+            const int lc = c - N.cell_base;
+            const int cz = lc / N.nxy;
+            const int cy = (lc - cz * N.nxy) / N.nx;
+            const int cx = lc - cz * N.nxy - cy * N.nx;
+            if (!list_runs(R, N, c, cz, cy, cx, runs, nr)) nr = -1; /* row by row, below */
+        }
+        s_nr[grp] = nr;
+    }
+    __syncwarp(); /* a group's lanes share a warp */
+    const int nr = s_nr[grp];
+    int total = 0;
+    for (int r = 0; r < nr; ++r) total += runs[r].y;
+    const int rounds = __reduce_max_sync(0xffffffffu, (total + G - 1) / G);
+    double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
+    int4 bi = make_int4(0, 0, 0, 0);
+    if (nr > 0) {
+        pi = R.pos[i];
+        bi = R.binfo[i];
+    }
+    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    const unsigned below = (1u << lane) - 1u;
+    int* __restrict__ out = R.list + (i >= 0 ? i : 0);
+    int n = 0;
+    int r = 0, off = gl; /* this lane's candidate: offset off in run r */
+    while (r < nr && off >= runs[r].y) off -= runs[r++].y;
+    for (int k = 0; k < rounds; ++k) {
+        bool acc = false;
+        int j = -1;
+        if (r < nr) {
+            j = R.cell_beads[runs[r].x + off];
+            if (j != i) {
+                const double4 pj = R.pos[j];
+                double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+                double length = rx * rx + ry * ry + rz * rz;
+                if (N.list_mi) length = min_image(N, rx, ry, rz, length, N.list_mi);
+                acc = length < N.list_r2_max && list_accept(N, R.pairs, length, pi, bi, pj, R.binfo[j]);
+            }
+        }
+        const unsigned mine = __ballot_sync(0xffffffffu, acc) & gmask;
+        if (acc) {
+            const int pos = n + __popc(mine & below);
+            if (pos < R.list_cap) out[(size_t)pos * R.list_stride] = j;
+        }
+        n += __popc(mine);
+        off += G;
+        while (r < nr && off >= runs[r].y) off -= runs[r++].y;
+    }
+    if (gl == 0 && i >= 0) {
+        if (nr < 0) {
+            list_one_bead(R, N, i, c);
+        } else {
+            if (n > R.list_cap)
+                atomicAdd(R.counters + FN_CNT_LIST_OVERFLOW, (unsigned long long)(n - R.list_cap));
+            R.list_count[i] = n;
+        }
+    }
 }
 
 /* Bead i's full list, reading its candidates from global memory (k_lists,
@@ -2133,6 +2267,8 @@ cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, 
     }
     if (R.bricks) {
         if (R.nbricks > 0) k_lists_brick<<<R.nbricks, kBrickThreads, 0, s>>>(R, R.bricks);
+    } else if (nb > 0 && R.list_lanes == 8) {
+        k_lists_group<8><<<(nb + 15) / 16, 128, 0, s>>>(R, ncells);
     } else if (nb > 0) {
         /* every bead may sit in the grid; threads past the grid total return */
         k_lists<<<(nb + 127) / 128, 128, 0, s>>>(R, ncells);

@@ -215,6 +215,9 @@ struct RebuildArgs {
        the per-bead list build) */
     const int4* bricks;
     int nbricks;
+    /* lanes per bead of the grouped list build (k_lists_group), 0: one
+       thread per bead (k_lists) */
+    int list_lanes;
     /* tile-compacted copy of the list for the staged step kernel (null: none) */
     int* csr;
     long long csr_region;

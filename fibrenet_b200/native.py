@@ -56,7 +56,8 @@ class FnStats(C.Structure):
                 ("bond_path", C.c_int), ("n_networks", C.c_int), ("n_beads", C.c_longlong),
                 ("device_bytes", C.c_longlong), ("graph_launches", C.c_longlong),
                 ("nonfinite", C.c_longlong), ("items_per_thread", C.c_int),
-                ("stalls", C.c_longlong), ("upload_on_device", C.c_int), ("list_by_bricks", C.c_int)]
+                ("stalls", C.c_longlong), ("upload_on_device", C.c_int), ("list_by_bricks", C.c_int),
+                ("list_build", C.c_int)]
 
 
 class FnView(C.Structure):
@@ -445,9 +446,14 @@ class Simulation:
         contact items per thread and round (0: no staging)."""
         self._check(self.lib.fn_set_kernel_shape(self.h, int(block), int(items_per_thread)))
 
-    def set_list_build(self, bricks: bool) -> None:
-        """Contact lists by bricks of cells (True) or bead by bead (False, the default)."""
-        self._check(self.lib.fn_set_list_build(self.h, int(bool(bricks))))
+    LIST_BUILDS = ("beads", "bricks", "groups")
+
+    def set_list_build(self, mode) -> None:
+        """How contact lists are built: "beads" (one thread per bead, the
+        default; also False / 0), "bricks" (cells staged in shared memory;
+        also True / 1) or "groups" (8 lanes per bead; also 2)."""
+        m = self.LIST_BUILDS.index(mode) if isinstance(mode, str) else int(mode)
+        self._check(self.lib.fn_set_list_build(self.h, m))
 
     def autotune(self, steps_per_trial: int = 20) -> int:
         self._check(self.lib.fn_autotune(self.h, steps_per_trial))

@@ -159,6 +159,8 @@ typedef struct fn_stats {
                                   converted the model on the device */
     int list_by_bricks;        /* 1: contact lists built by bricks of cells
                                   (fn_set_list_build) */
+    int list_build;            /* the list build in use: 0 bead by bead, 1 by
+                                  bricks of cells, 2 by groups of lanes */
 } fn_stats;
 
 /* A device array of the context, for zero-copy readers (torch through
@@ -357,16 +359,17 @@ FN_API int fn_device_view(fn_ctx* ctx, int field, fn_view* out);
    (block size 64 .. 512; for the staged chain kernel also 2, 4 or 8 contact
    items per thread and round, or no staging) from one snapshot of the state,
    restored after every trial, keeps the fastest, then keeps the faster of the
-   two list builds (fn_set_list_build) at that shape; the simulation does not
+   list builds (fn_set_list_build) at that shape; the simulation does not
    advance. */
 FN_API int fn_autotune(fn_ctx* ctx, int steps_per_trial);
 
 /* How contact lists are built (ResetGrid .. BuildContactList,
-   kernel.cl:487-789): 1 by bricks of 8 x 4 x 4 grid cells whose beads and
-   neighbouring beads are staged in shared memory, 0 (the default) bead by
-   bead from global memory.  Both give the same lists, entry for entry;
-   fn_autotune keeps the faster. */
-FN_API int fn_set_list_build(fn_ctx* ctx, int bricks);
+   kernel.cl:487-789): 0 (the default) one thread per bead reading its
+   candidates from global memory; 1 by bricks of 8 x 4 x 4 grid cells whose
+   beads and neighbouring beads are staged in shared memory; 2 by groups of 8
+   lanes per bead (more threads in flight for small networks).  All give the
+   same lists, entry for entry; fn_autotune keeps the fastest. */
+FN_API int fn_set_list_build(fn_ctx* ctx, int mode);
 
 /* Sets the step kernel's shape: threads per block (a multiple of 32; 64 ..
    256 on the chain path, whose tiles hold block - 4 beads) and, for the

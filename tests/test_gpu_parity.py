@@ -363,11 +363,12 @@ def test_state_save_restore_repeats_steps():
 
 
 @pytest.mark.parametrize("kind", ["tensile", "dense_periodic", "small_grid", "full_cells"])
-def test_brick_lists_equal_bead_lists(kind):
-    """The list build by bricks of cells gives the per-bead build's lists,
-    entry for entry (same order), on finite and periodic boxes, a grid of
-    three cells per axis (every halo wraps onto itself) and cells fuller
-    than the cell capacity; and the same trajectory."""
+def test_list_builds_equal_bead_lists(kind):
+    """The list builds by bricks of cells and by groups of lanes give the
+    per-bead build's lists, entry for entry (same order), on finite and
+    periodic boxes, a grid of three cells per axis (every halo wraps onto
+    itself) and cells fuller than the cell capacity; and the same
+    trajectory."""
     cell_cap = 64
     if kind == "tensile":
         m = g.tensile_network(seed=33, fibres=300, beads=40, box=(120.0, 90.0, 12.0), z_range=(1.0, 11.0),
@@ -379,19 +380,28 @@ def test_brick_lists_equal_bead_lists(kind):
     else:
         m = g.plain_network(seed=35, fibres=60, beads=20, box=(6.0, 6.0, 4.0), z_range=(0.5, 3.5))
         cell_cap = 6
-    a = sim(m, list_capacity=64, cell_capacity=cell_cap, reorder=True)
     b = sim(m, list_capacity=64, cell_capacity=cell_cap, reorder=True)
-    b.set_list_build(False)
+    b.set_list_build("beads")
+    assert b.stats()["list_build"] == 0
+    builds = {mode: sim(m, list_capacity=64, cell_capacity=cell_cap, reorder=True)
+              for mode in ("bricks", "groups")}
+    for mode, a in builds.items():
+        a.set_list_build(mode)
+        assert a.stats()["list_build"] == ("beads", "bricks", "groups").index(mode)
     for n in (1, 8, 17):
-        a.step(n)
         b.step(n)
-        ca, pa = a.lists()
         cb, pb = b.lists()
-        np.testing.assert_array_equal(ca, cb)
-        np.testing.assert_array_equal(pa, pb)
-        assert a.stats()["list_overflow"] == b.stats()["list_overflow"]
-        assert a.stats()["cell_overflow"] == b.stats()["cell_overflow"]
-    for f in FIELDS:
-        np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f)
+        for mode, a in builds.items():
+            a.step(n)
+            ca, pa = a.lists()
+            np.testing.assert_array_equal(ca, cb, err_msg=mode)
+            np.testing.assert_array_equal(pa, pb, err_msg=mode)
+            assert a.stats()["list_overflow"] == b.stats()["list_overflow"], mode
+            assert a.stats()["cell_overflow"] == b.stats()["cell_overflow"], mode
+    for mode, a in builds.items():
+        for f in FIELDS:
+            np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f"{mode} {f}")
+        a.close()
     if kind == "full_cells":
-        assert a.stats()["cell_overflow"] > 0
+        assert b.stats()["cell_overflow"] > 0
+    b.close()
