@@ -1282,6 +1282,7 @@ __global__ void k_cells(const RebuildArgs R) {
         atomicAdd(R.cell_count + cell, 1);
     }
     R.cell_of[i] = cell;
+    R.list_count[i] = 0; /* k_lists counts only the beads it lists */
 }
 
 __global__ void k_scatter(const RebuildArgs R, int nb) {
@@ -1959,9 +1960,11 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int* block_sums, int
     if (threadIdx.x == 0) *grand_total = carry;
 }
 
+/* Exclusive scan, last pass: each block's offset added, written to out;
+   zero (if given) is cleared alongside, sparing a launch. */
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int* in, long long n,
                                                               const int* block_sums, int* out,
-                                                              const int* gate) {
+                                                              const int* gate, int* zero) {
     FN_GATED(gate);
     __shared__ int ws[33];
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
@@ -1976,7 +1979,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int* in, long
     int ex = block_exclusive_scan(s, ws, total) + block_sums[blockIdx.x];
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; ++k) {
-        if (base + k < n) out[base + k] = ex;
+        if (base + k < n) {
+            out[base + k] = ex;
+            if (zero) zero[base + k] = 0;
+        }
         ex += v[k];
     }
 }
@@ -2237,7 +2243,7 @@ cudaError_t launch_exclusive_scan(const int* in, long long n, int* out, int* blo
     const long long nblk = scan_block_count(n);
     k_scan_partials<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(in, n, block_sums, nullptr);
     k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(block_sums, (int)nblk, out + n, nullptr);
-    k_scan_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(in, n, block_sums, out, nullptr);
+    k_scan_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(in, n, block_sums, out, nullptr, nullptr);
     return cudaGetLastError();
 }
 
@@ -2245,26 +2251,20 @@ cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, 
                            int* scan_block_sums, cudaStream_t s) {
     cudaError_t e;
     const unsigned fill_blocks = (unsigned)std::min<long long>(4096, (ncells + 255) / 256 + 1);
-    if (R.gate) {
+    /* cell fills are cleared by the scan's last pass and list counts by
+       k_cells, so only the cell counts need a pass of their own */
+    if (R.gate)
         k_fill_int<<<fill_blocks, 256, 0, s>>>(R.cell_count, ncells, 0, R.gate);
-        k_fill_int<<<fill_blocks, 256, 0, s>>>(R.cell_fill, ncells, 0, R.gate);
-    } else {
-        if ((e = cudaMemsetAsync(R.cell_count, 0, sizeof(int) * (size_t)ncells, s))) return e;
-        if ((e = cudaMemsetAsync(R.cell_fill, 0, sizeof(int) * (size_t)ncells, s))) return e;
-    }
+    else if ((e = cudaMemsetAsync(R.cell_count, 0, sizeof(int) * (size_t)ncells, s)))
+        return e;
     if (ntiles > 0) k_cells<<<ntiles, block, 0, s>>>(R);
     const long long nblk = scan_block_count(ncells);
     k_scan_partials<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums, R.gate);
     k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(scan_block_sums, (int)nblk, R.cell_start + ncells, R.gate);
     k_scan_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums,
-                                                          R.cell_start, R.gate);
+                                                          R.cell_start, R.gate, R.cell_fill);
     if (nb > 0) k_scatter<<<(nb + 255) / 256, 256, 0, s>>>(R, nb);
     k_cell_sort<<<(unsigned)((ncells + 255) / 256), 256, 0, s>>>(R, (int)ncells);
-    if (R.gate) {
-        if (nb > 0) k_fill_int<<<(unsigned)std::min(4096, (nb + 255) / 256), 256, 0, s>>>(R.list_count, nb, 0, R.gate);
-    } else {
-        if ((e = cudaMemsetAsync(R.list_count, 0, sizeof(int) * (size_t)nb, s))) return e;
-    }
     if (R.bricks) {
         if (R.nbricks > 0) k_lists_brick<<<R.nbricks, kBrickThreads, 0, s>>>(R, R.bricks);
     } else if (nb > 0 && R.list_lanes == 8) {
