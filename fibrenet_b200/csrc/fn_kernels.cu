@@ -1987,6 +1987,41 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int* in, long
     }
 }
 
+/* Exclusive scan, last pass, without a pass of its own over the block sums:
+   each block adds up the raw sums of the blocks before it (a few thousand at
+   most, read from L2), the last block writes the grand total; zero (if
+   given) is cleared alongside. */
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply_direct(const int* in, long long n,
+                                                                     const int* block_sums, int nblocks,
+                                                                     int* out, int* grand_total,
+                                                                     const int* gate, int* zero) {
+    FN_GATED(gate);
+    __shared__ int ws[33];
+    int before = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += SCAN_THREADS) before += block_sums[b];
+    int offset;
+    block_exclusive_scan(before, ws, offset); /* offset: the block sums' total */
+    const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        s += v[k];
+    }
+    int total;
+    int ex = block_exclusive_scan(s, ws, total) + offset;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        if (base + k < n) {
+            out[base + k] = ex;
+            if (zero) zero[base + k] = 0;
+        }
+        ex += v[k];
+    }
+    if (blockIdx.x == nblocks - 1 && threadIdx.x == 0) *grand_total = offset + total;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Observables: deterministic two-pass FP64 reduction per network.           */
 
@@ -2260,9 +2295,9 @@ cudaError_t launch_rebuild(const RebuildArgs& R, int ntiles, int block, int nb, 
     if (ntiles > 0) k_cells<<<ntiles, block, 0, s>>>(R);
     const long long nblk = scan_block_count(ncells);
     k_scan_partials<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums, R.gate);
-    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(scan_block_sums, (int)nblk, R.cell_start + ncells, R.gate);
-    k_scan_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums,
-                                                          R.cell_start, R.gate, R.cell_fill);
+    k_scan_apply_direct<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(R.cell_count, ncells, scan_block_sums, (int)nblk,
+                                                                 R.cell_start, R.cell_start + ncells, R.gate,
+                                                                 R.cell_fill);
     if (nb > 0) k_scatter<<<(nb + 255) / 256, 256, 0, s>>>(R, nb);
     k_cell_sort<<<(unsigned)((ncells + 255) / 256), 256, 0, s>>>(R, (int)ncells);
     if (R.bricks) {
