@@ -358,9 +358,9 @@ FN_API int fn_device_view(fn_ctx* ctx, int field, fn_view* out);
 /* Times steps_per_trial steps at each candidate shape of the step kernel
    (block size 64 .. 512; for the staged chain kernel also 2, 4 or 8 contact
    items per thread and round, or no staging) from one snapshot of the state,
-   restored after every trial, keeps the fastest, then keeps the faster of the
-   list builds (fn_set_list_build) at that shape; the simulation does not
-   advance. */
+   restored after every trial, keeps the fastest, then keeps the fastest of
+   the three list builds (fn_set_list_build) at that shape; the simulation
+   does not advance. */
 FN_API int fn_autotune(fn_ctx* ctx, int steps_per_trial);
 
 /* How contact lists are built (ResetGrid .. BuildContactList,
